@@ -1,0 +1,172 @@
+/* depth_cuda: B200 (sm_100a) stereo-depth hot path behind a plain C ABI.
+ *
+ * The stages: rectification remap of a raw IR pair -> 5x5 (configurable) census -> Hamming matching
+ * cost -> multi-path SGM with P1/P2 -> winner-takes-all with subpixel fit -> left/right check ->
+ * 3x3 median -> disparity-to-depth. It is a drop-in for the reference's GPU stereo matcher
+ * (libs/depth_metal/include/einstar/depth_metal/metal_stereo.hpp:67-107, class MetalStereo), which
+ * implements libs/depth's matcher interface (libs/depth/include/einstar/depth/stereo.hpp:96-115).
+ *
+ * Conventions
+ * - Every entry point returns an int status with the values of einstar::Errc
+ *   (libs/core/include/einstar/core/error.hpp:8-19); the message of the last failure is available from
+ *   ds_last_error() (per handle) or ds_last_global_error() (create failures, per thread).
+ * - Host images are u8 rows `stride` bytes apart (stride >= width); outputs are tightly packed.
+ * - A handle is not thread-safe (as MetalStereo: callers serialise per handle). It owns all its device
+ *   buffers and one CUDA stream.
+ * - Disparities follow the reference: d = x_left - x_right, float, -1e9 where invalid
+ *   (stereo.hpp:23-24). The u16 output is round((d - min_disparity) * 64), 0xFFFF where invalid.
+ */
+#ifndef DEPTH_CUDA_H
+#define DEPTH_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DS_API __attribute__((visibility("default")))
+#else
+#define DS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* einstar::Errc (libs/core/include/einstar/core/error.hpp:8-19), same values. */
+enum ds_status {
+    DS_OK = 0,
+    DS_NOT_FOUND = 1,
+    DS_IO = 2,
+    DS_TIMEOUT = 3,
+    DS_PROTOCOL = 4,
+    DS_INVALID_ARGUMENT = 5,
+    DS_BLOCKED = 6,
+    DS_UNSUPPORTED = 7,
+    DS_BUSY = 8,
+    DS_DISCONNECTED = 9
+};
+
+/* depth::SgmParams (libs/depth/include/einstar/depth/stereo.hpp:26-40); ints for bools. */
+typedef struct ds_sgm_params {
+    int min_disparity;
+    int num_disparities; /* 1..512 */
+    int census_radius_x; /* window (2rx+1) <= 9 */
+    int census_radius_y; /* window (2ry+1) <= 7 */
+    int p1;
+    int p2;
+    int adaptive_p2;
+    int eight_paths;
+    int slant_steps;
+    float uniqueness;
+    int lr_max_diff;
+} ds_sgm_params;
+
+/* depth::StereoParams (stereo.hpp:80-88) reduced to the hot path. The stages after SGM that this
+ * library does not run (pyramid + ZNCC refinement, detail refinement, occlusion / spike filters,
+ * speckle removal) keep their switches so that a caller asking for them gets DS_UNSUPPORTED instead
+ * of silently different results. */
+typedef struct ds_stereo_params {
+    int pyramid_levels;          /* must be 0 */
+    ds_sgm_params sgm;
+    int subpixel;                /* parabola fit in the WTA (stereo.cpp:430-431) */
+    int median;                  /* 3x3 median of valid neighbours after the L-R check (stereo.cpp:129-147) */
+    int detail_enabled;          /* must be 0 */
+    int filter_occlusion;        /* must be 0 */
+    int filter_spikes;           /* must be 0 */
+    int speckle_max_region_size; /* must be 0 */
+    int wide_costs;              /* 1: 16-bit path values even when census window + P2 <= 255 */
+} ds_stereo_params;
+
+/* depth::RectifiedGeometry (libs/depth/include/einstar/depth/point_image.hpp:12-26). */
+typedef struct ds_geometry {
+    double f;
+    double cx, cy;
+    double baseline;
+    double cx_offset;
+} ds_geometry;
+
+/* depth_metal::StereoTimings (metal_stereo.hpp:61-65). */
+typedef struct ds_timings {
+    double gpu_ms;     /* device time of the frame's work (CUDA events on the handle's stream) */
+    double speckle_ms; /* always 0: no CPU speckle stage */
+    double total_ms;   /* host wall time of the call */
+} ds_timings;
+
+/* Output slots of one frame; every pointer may be NULL (not produced). Host memory for
+ * ds_compute / ds_compute_raw, device memory for the *_device variants. */
+typedef struct ds_outputs {
+    float* disparity;        /* W*H f32, after L-R check (+ median when enabled) */
+    float* confidence;       /* W*H f32, 1 where the disparity is valid, else 0 (stereo.cpp:515-519) */
+    uint16_t* disparity_u16; /* W*H u16 (see above) */
+    float* depth;            /* W*H f32 mm, 0 where invalid or outside [min_depth, max_depth]; needs ds_set_point_params */
+    uint8_t* rect_left;      /* W*H u8 rectified images (compute_raw only) */
+    uint8_t* rect_right;
+} ds_outputs;
+
+typedef struct ds_handle ds_handle;
+
+/* Hot-path defaults: depth::SgmParams defaults, pyramid 0, subpixel and median on, other stages off. */
+DS_API void ds_default_params(ds_stereo_params* params);
+
+/* MetalStereo::create (metal_stereo.hpp:70-71; validation as metal_stereo.cpp:115-120). */
+DS_API int ds_create(const ds_stereo_params* params, int width, int height, ds_handle** out);
+DS_API void ds_destroy(ds_handle* handle);
+
+/* MetalStereo::set_rectification (metal_stereo.hpp:75): float32 remap tables (map_x, map_y per camera,
+ * map_width x map_height, tightly packed) copied to the device once and kept resident. The tables
+ * are either at the stereo resolution (full-resolution SGM) or twice it, in which case the rectified
+ * image is box-downsampled 2x2 as calib::remap + depth::downsample2 would give. */
+DS_API int ds_set_rectification(ds_handle* handle, const float* map_left_x, const float* map_left_y,
+                                 const float* map_right_x, const float* map_right_y, int map_width, int map_height,
+                                 int raw_width, int raw_height);
+
+/* MetalStereo::set_point_params (metal_stereo.hpp:84-85). */
+DS_API int ds_set_point_params(ds_handle* handle, const ds_geometry* geometry, float min_depth_mm, float max_depth_mm,
+                               float max_depth_jump_mm);
+
+/* MetalStereo::compute (metal_stereo.hpp:78): already rectified pair, host memory. */
+DS_API int ds_compute(ds_handle* handle, const uint8_t* left, const uint8_t* right, ptrdiff_t stride,
+                      const ds_outputs* out);
+
+/* MetalStereo::compute_raw (metal_stereo.hpp:80-81): raw pair (raw_width x raw_height), host memory. */
+DS_API int ds_compute_raw(ds_handle* handle, const uint8_t* raw_left, const uint8_t* raw_right, ptrdiff_t stride,
+                          const ds_outputs* out);
+
+/* Device-resident variants (no counterpart in the reference, whose buffers live in unified memory):
+ * inputs and outputs are device pointers (tightly packed), the work is enqueued on `stream`
+ * (a cudaStream_t; NULL = the handle's own stream) and the call returns without waiting. */
+DS_API int ds_compute_device(ds_handle* handle, const uint8_t* left, const uint8_t* right, const ds_outputs* out,
+                             void* stream);
+DS_API int ds_compute_raw_device(ds_handle* handle, const uint8_t* raw_left, const uint8_t* raw_right,
+                                 const ds_outputs* out, void* stream);
+
+/* MetalStereo::last_timings (metal_stereo.hpp:97). */
+DS_API int ds_last_timings(const ds_handle* handle, ds_timings* out);
+DS_API const char* ds_last_error(const ds_handle* handle);
+DS_API const char* ds_last_global_error(void);
+
+/* Intermediate results of the last frame, for stage-by-stage parity tests (host memory, may be NULL):
+ * census words (u64, W*H each) and the summed path costs (u16, H*W*num_disparities, [y][x][d]). */
+DS_API int ds_debug_read(ds_handle* handle, uint64_t* census_left, uint64_t* census_right, uint16_t* path_sums);
+
+/* Device bytes the handle holds (all buffers). */
+DS_API size_t ds_device_bytes(const ds_handle* handle);
+
+/* Per-stage device times, the counterpart of the reference's per-stage GPU profile
+ * (libs/gpu/include/einstar/gpu/profile.hpp:14-32; stage labels metal_stereo.cpp:480-652). When enabled,
+ * every frame records CUDA events between its stages on the stream it runs on; nothing is serialised.
+ * Stages: 0 rectify, 1 census, 2 SGM paths, 3 WTA + L-R check, 4 median + outputs (DS_STAGES). */
+#define DS_STAGES 5
+DS_API int ds_profile_enable(ds_handle* handle, int on);
+/* Waits for the profiled frames since the last call and writes up to `max_frames` rows of DS_STAGES
+ * milliseconds each to `stage_ms` (row = frame, oldest first); `*frames` = rows written. */
+DS_API int ds_profile_collect(ds_handle* handle, double* stage_ms, int max_frames, int* frames);
+
+/* Number of kernels this library has launched since it was loaded (all handles). */
+DS_API uint64_t ds_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DEPTH_CUDA_H */

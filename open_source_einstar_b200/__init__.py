@@ -1,0 +1,19 @@
+"""B200-native stereo-depth hot path of the Einstar scanner pipeline.
+
+rectify -> census -> Hamming cost -> multi-path SGM -> WTA + subpixel -> L-R check -> 3x3 median ->
+depth, as hand-written sm_100a CUDA behind the C ABI in include/depth_cuda.h (libdepth_cuda.so).
+The Python classes mirror the reference's stereo-matcher interface (depth_metal::MetalStereo).
+"""
+from .stereo import (  # noqa: F401
+    INVALID_DISPARITY,
+    CudaStereo,
+    Errc,
+    RectifiedGeometry,
+    RemapTable,
+    SgmParams,
+    StereoError,
+    StereoParams,
+    StereoResult,
+    StereoTimings,
+    valid_disparity,
+)

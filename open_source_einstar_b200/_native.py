@@ -1,0 +1,84 @@
+"""ctypes binding of include/depth_cuda.h (libdepth_cuda.so). No torch types cross the boundary.
+
+The library is the product path. There is no fallback: if it is missing or cannot be loaded, import
+of the stereo classes raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .build import LIB
+
+
+class SgmParamsC(C.Structure):
+    _fields_ = [
+        ("min_disparity", C.c_int), ("num_disparities", C.c_int),
+        ("census_radius_x", C.c_int), ("census_radius_y", C.c_int),
+        ("p1", C.c_int), ("p2", C.c_int), ("adaptive_p2", C.c_int),
+        ("eight_paths", C.c_int), ("slant_steps", C.c_int),
+        ("uniqueness", C.c_float), ("lr_max_diff", C.c_int),
+    ]
+
+
+class StereoParamsC(C.Structure):
+    _fields_ = [
+        ("pyramid_levels", C.c_int), ("sgm", SgmParamsC), ("subpixel", C.c_int), ("median", C.c_int),
+        ("detail_enabled", C.c_int), ("filter_occlusion", C.c_int), ("filter_spikes", C.c_int),
+        ("speckle_max_region_size", C.c_int), ("wide_costs", C.c_int),
+    ]
+
+
+class GeometryC(C.Structure):
+    _fields_ = [("f", C.c_double), ("cx", C.c_double), ("cy", C.c_double), ("baseline", C.c_double),
+                ("cx_offset", C.c_double)]
+
+
+class TimingsC(C.Structure):
+    _fields_ = [("gpu_ms", C.c_double), ("speckle_ms", C.c_double), ("total_ms", C.c_double)]
+
+
+class OutputsC(C.Structure):
+    _fields_ = [("disparity", C.c_void_p), ("confidence", C.c_void_p), ("disparity_u16", C.c_void_p),
+                ("depth", C.c_void_p), ("rect_left", C.c_void_p), ("rect_right", C.c_void_p)]
+
+
+# Every symbol include/depth_cuda.h declares: name -> (restype, argtypes).
+_vp, _i, _f, _sz = C.c_void_p, C.c_int, C.c_float, C.c_size_t
+SIGNATURES = {
+    "ds_default_params": (None, [C.POINTER(StereoParamsC)]),
+    "ds_create": (_i, [C.POINTER(StereoParamsC), _i, _i, C.POINTER(_vp)]),
+    "ds_destroy": (None, [_vp]),
+    "ds_set_rectification": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i]),
+    "ds_set_point_params": (_i, [_vp, C.POINTER(GeometryC), _f, _f, _f]),
+    "ds_compute": (_i, [_vp, _vp, _vp, C.c_ssize_t, C.POINTER(OutputsC)]),
+    "ds_compute_raw": (_i, [_vp, _vp, _vp, C.c_ssize_t, C.POINTER(OutputsC)]),
+    "ds_compute_device": (_i, [_vp, _vp, _vp, C.POINTER(OutputsC), _vp]),
+    "ds_compute_raw_device": (_i, [_vp, _vp, _vp, C.POINTER(OutputsC), _vp]),
+    "ds_last_timings": (_i, [_vp, C.POINTER(TimingsC)]),
+    "ds_last_error": (C.c_char_p, [_vp]),
+    "ds_last_global_error": (C.c_char_p, []),
+    "ds_debug_read": (_i, [_vp, _vp, _vp, _vp]),
+    "ds_device_bytes": (_sz, [_vp]),
+    "ds_profile_enable": (_i, [_vp, _i]),
+    "ds_profile_collect": (_i, [_vp, _vp, _i, C.POINTER(_i)]),
+    "ds_kernel_launches": (C.c_uint64, []),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libdepth_cuda.so (in-tree); raises if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            raise ImportError(f"{LIB} is not built: run open_source_einstar_b200.build.build_native() "
+                              "(or __graft_entry__.build()); there is no CPU fallback")
+        L = C.CDLL(LIB)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib

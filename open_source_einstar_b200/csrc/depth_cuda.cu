@@ -1,0 +1,649 @@
+// C-ABI of the per-frame stereo hot path (include/depth_cuda.h): handle life cycle, validation with
+// the reference's error codes, resident rectification tables, host and device entry points.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/depth_cuda.h"
+#include "stereo_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_error;
+std::atomic<uint64_t> g_launches{0};
+
+constexpr int kProfileRing = 256;  // frames whose stage events can be pending at once
+
+struct CudaFailure {
+    cudaError_t err;
+    const char* what;
+};
+
+#define DS_CUDA(call)                                           \
+    do {                                                        \
+        const cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) throw CudaFailure{e_, #call};    \
+    } while (0)
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int round_vpl(int nd) {
+    const int need = (nd + 31) / 32;
+    static const int kSteps[] = {1, 2, 3, 4, 6, 8, 12, 16};
+    for (int s : kSteps)
+        if (s >= need) return s;
+    return 16;
+}
+
+}  // namespace
+
+struct ds_handle {
+    ds_stereo_params p{};
+    int w = 0, h = 0;
+    int nd = 0, vpl = 0, dp = 0, ndirs = 4;
+    bool wide = false;      // u16 path values
+    bool census64 = false;  // u64 census words
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    uint8_t* d_rect[2] = {nullptr, nullptr};
+    uint8_t* d_raw[2] = {nullptr, nullptr};
+    float* d_map[4] = {nullptr, nullptr, nullptr, nullptr};  // lx, ly, rx, ry
+    int map_w = 0, map_h = 0, raw_w = 0, raw_h = 0;
+    bool have_rect = false;
+    void* d_census[2] = {nullptr, nullptr};
+    void* d_values = nullptr;
+    size_t dir_stride = 0;
+    float* d_disp_lr = nullptr;
+    float* d_out_disp = nullptr;
+    float* d_out_conf = nullptr;
+    uint16_t* d_out_u16 = nullptr;
+    float* d_out_depth = nullptr;
+
+    ds_geometry geom{};
+    float min_depth = 150.0f, max_depth = 700.0f, max_jump = 4.0f;
+    bool have_points = false;
+
+    ds_timings timings{};
+    std::string err;
+    size_t bytes = 0;
+
+    // Stage profiling: a ring of (DS_STAGES + 1) events per frame.
+    bool profile = false;
+    std::vector<cudaEvent_t> prof_events;
+    int prof_head = 0, prof_pending = 0;
+
+    int fail(int code, std::string msg) {
+        err = std::move(msg);
+        return code;
+    }
+    template <typename T>
+    T* alloc(size_t n) {
+        void* p = nullptr;
+        DS_CUDA(cudaMalloc(&p, n * sizeof(T)));
+        bytes += n * sizeof(T);
+        return static_cast<T*>(p);
+    }
+};
+
+namespace {
+
+void release(ds_handle* h) {
+    if (!h) return;
+    auto f = [](void* p) {
+        if (p) cudaFree(p);
+    };
+    for (auto* p : h->d_rect) f(p);
+    for (auto* p : h->d_raw) f(p);
+    for (auto* p : h->d_map) f(p);
+    for (auto* p : h->d_census) f(p);
+    f(h->d_values);
+    f(h->d_disp_lr);
+    f(h->d_out_disp);
+    f(h->d_out_conf);
+    f(h->d_out_u16);
+    f(h->d_out_depth);
+    for (auto e : h->prof_events) cudaEventDestroy(e);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+// Validation of metal_stereo.cpp:115-120, plus the limits of this implementation.
+int validate(const ds_stereo_params& p, int w, int h, std::string& msg) {
+    const auto& s = p.sgm;
+    if (w < 1 || h < 1 || w > 16384 || h > 16384) {
+        msg = "image size must be 1..16384 in each dimension";
+        return DS_INVALID_ARGUMENT;
+    }
+    if (s.num_disparities < 1 || s.num_disparities > dsk::kMaxDisparities) {
+        msg = "CUDA SGM supports 1..512 disparities";
+        return DS_INVALID_ARGUMENT;
+    }
+    if (s.census_radius_x < 0 || s.census_radius_y < 0 || s.census_radius_x * 2 + 1 > 9 || s.census_radius_y * 2 + 1 > 7) {
+        msg = "census window too large for 64 bits";
+        return DS_INVALID_ARGUMENT;
+    }
+    if (s.p1 < 0 || s.p2 < 0) {
+        msg = "SGM penalties must be non-negative";
+        return DS_INVALID_ARGUMENT;
+    }
+    const int window = (2 * s.census_radius_x + 1) * (2 * s.census_radius_y + 1);
+    if (window + s.p2 > 0xFFFF - 2 * s.p1) {
+        msg = "census window + P2 exceed the 16-bit SGM costs";
+        return DS_INVALID_ARGUMENT;
+    }
+    if (p.pyramid_levels != 0) {
+        msg = "pyramid + ZNCC refinement is not part of the CUDA hot path (pyramid_levels must be 0)";
+        return DS_UNSUPPORTED;
+    }
+    if (p.detail_enabled || p.filter_occlusion || p.filter_spikes || p.speckle_max_region_size > 0) {
+        msg = "detail refinement, occlusion/spike filters and speckle removal are not part of the CUDA hot path";
+        return DS_UNSUPPORTED;
+    }
+    return DS_OK;
+}
+
+template <int VPL, typename CW, typename ST>
+void launch_paths_t(const ds_handle* h, cudaStream_t st) {
+    dsk::PathArgs a{};
+    a.census_l = h->d_census[0];
+    a.census_r = h->d_census[1];
+    a.guide = h->d_rect[0];
+    a.values = h->d_values;
+    a.dir_stride = h->dir_stride;
+    a.w = h->w;
+    a.h = h->h;
+    a.nd = h->nd;
+    a.dp = h->dp;
+    a.min_disp = h->p.sgm.min_disparity;
+    a.p1 = h->p.sgm.p1;
+    a.invalid_cost = (2 * h->p.sgm.census_radius_x + 1) * (2 * h->p.sgm.census_radius_y + 1);
+    a.slant = h->p.sgm.slant_steps ? 1 : 0;
+    a.dir_base = 0;
+    for (int q = 0; q < 32; ++q) {
+        const int adaptive = std::max(h->p.sgm.p1 + 1, h->p.sgm.p2 / (q + 1));
+        a.p2_table[q] = h->p.sgm.adaptive_p2 ? adaptive : h->p.sgm.p2;
+    }
+    const int wpb = 4;
+    const int max_lines = h->ndirs == 8 ? h->w + h->h - 1 : std::max(h->w, h->h);
+    dim3 grid((max_lines + wpb - 1) / wpb, h->ndirs);
+    dsk::k_paths<VPL, CW, ST><<<grid, wpb * 32, 0, st>>>(a);
+}
+
+template <int VPL, typename ST>
+void launch_wta_t(const ds_handle* h, cudaStream_t st) {
+    dsk::WtaArgs a{};
+    a.values = h->d_values;
+    a.dir_stride = h->dir_stride;
+    a.ndirs = h->ndirs;
+    a.w = h->w;
+    a.h = h->h;
+    a.nd = h->nd;
+    a.dp = h->dp;
+    a.min_disp = h->p.sgm.min_disparity;
+    a.uniqueness = h->p.sgm.uniqueness;
+    a.subpixel = h->p.subpixel ? 1 : 0;
+    a.lr_max_diff = h->p.sgm.lr_max_diff;
+    a.disp = h->d_disp_lr;
+    const size_t smem = static_cast<size_t>(h->w) * 8;
+    DS_CUDA(cudaFuncSetAttribute(dsk::k_wta<VPL, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    dsk::k_wta<VPL, ST><<<h->h, 256, smem, st>>>(a);
+}
+
+template <int VPL>
+void paths_vpl(const ds_handle* h, cudaStream_t st) {
+    if (h->census64) {
+        if (h->wide) launch_paths_t<VPL, uint64_t, uint16_t>(h, st);
+        else launch_paths_t<VPL, uint64_t, uint8_t>(h, st);
+    } else {
+        if (h->wide) launch_paths_t<VPL, uint32_t, uint16_t>(h, st);
+        else launch_paths_t<VPL, uint32_t, uint8_t>(h, st);
+    }
+    ++g_launches;
+}
+
+template <int VPL>
+void wta_vpl(const ds_handle* h, cudaStream_t st) {
+    if (h->wide) launch_wta_t<VPL, uint16_t>(h, st);
+    else launch_wta_t<VPL, uint8_t>(h, st);
+    ++g_launches;
+}
+
+template <template <int> class Op>
+void by_vpl(const ds_handle* h, cudaStream_t st) {
+    switch (h->vpl) {
+        case 1: Op<1>::run(h, st); break;
+        case 2: Op<2>::run(h, st); break;
+        case 3: Op<3>::run(h, st); break;
+        case 4: Op<4>::run(h, st); break;
+        case 6: Op<6>::run(h, st); break;
+        case 8: Op<8>::run(h, st); break;
+        case 12: Op<12>::run(h, st); break;
+        default: Op<16>::run(h, st); break;
+    }
+}
+template <int V>
+struct PathsOp {
+    static void run(const ds_handle* h, cudaStream_t st) { paths_vpl<V>(h, st); }
+};
+template <int V>
+struct WtaOp {
+    static void run(const ds_handle* h, cudaStream_t st) { wta_vpl<V>(h, st); }
+};
+
+void launch_paths(const ds_handle* h, cudaStream_t st) { by_vpl<PathsOp>(h, st); }
+void launch_wta(const ds_handle* h, cudaStream_t st) { by_vpl<WtaOp>(h, st); }
+
+struct StageMarks {
+    ds_handle* h;
+    cudaStream_t st;
+    int slot = -1;
+    void mark(int i) {
+        if (slot >= 0) DS_CUDA(cudaEventRecord(h->prof_events[static_cast<size_t>(slot) * (DS_STAGES + 1) + i], st));
+    }
+};
+
+// The whole frame on `st`: [rectify] -> census -> paths -> WTA + L-R -> median + outputs.
+void enqueue_frame(ds_handle* h, const uint8_t* left, const uint8_t* right, bool raw, const ds_outputs& out,
+                   cudaStream_t st) {
+    const uint8_t* img[2] = {left, right};
+    StageMarks marks{h, st};
+    if (h->profile) {
+        if (h->prof_pending == kProfileRing) throw CudaFailure{cudaErrorNotReady, "profile ring full: call ds_profile_collect"};
+        marks.slot = (h->prof_head + h->prof_pending) % kProfileRing;
+        ++h->prof_pending;
+    }
+    marks.mark(0);
+    if (raw) {
+        dsk::RectifyArgs r{};
+        for (int s = 0; s < 2; ++s) {
+            r.raw[s] = img[s];
+            r.map_x[s] = h->d_map[2 * s];
+            r.map_y[s] = h->d_map[2 * s + 1];
+            r.out[s] = h->d_rect[s];
+        }
+        r.raw_w = h->raw_w;
+        r.raw_h = h->raw_h;
+        r.map_w = h->map_w;
+        r.out_w = h->w;
+        r.out_h = h->h;
+        r.half = h->map_w == 2 * h->w ? 1 : 0;
+        dim3 b(32, 8), g((h->w + 31) / 32, (h->h + 7) / 8, 2);
+        dsk::k_rectify<<<g, b, 0, st>>>(r);
+        ++g_launches;
+        img[0] = h->d_rect[0];
+        img[1] = h->d_rect[1];
+    } else if (left != h->d_rect[0]) {
+        // Device inputs of the caller: the path kernel reads the left image as its guide.
+        DS_CUDA(cudaMemcpyAsync(h->d_rect[0], left, static_cast<size_t>(h->w) * h->h, cudaMemcpyDeviceToDevice, st));
+        DS_CUDA(cudaMemcpyAsync(h->d_rect[1], right, static_cast<size_t>(h->w) * h->h, cudaMemcpyDeviceToDevice, st));
+        img[0] = h->d_rect[0];
+        img[1] = h->d_rect[1];
+    }
+    marks.mark(1);
+    {
+        dsk::CensusArgs c{};
+        c.img[0] = img[0];
+        c.img[1] = img[1];
+        c.out[0] = h->d_census[0];
+        c.out[1] = h->d_census[1];
+        c.w = h->w;
+        c.h = h->h;
+        c.rx = h->p.sgm.census_radius_x;
+        c.ry = h->p.sgm.census_radius_y;
+        dim3 b(32, 8), g((h->w + 31) / 32, (h->h + 7) / 8, 2);
+        if (h->census64) dsk::k_census<uint64_t><<<g, b, 0, st>>>(c);
+        else dsk::k_census<uint32_t><<<g, b, 0, st>>>(c);
+        ++g_launches;
+    }
+    marks.mark(2);
+    launch_paths(h, st);
+    marks.mark(3);
+    launch_wta(h, st);
+    marks.mark(4);
+    {
+        dsk::PostArgs q{};
+        q.disp = h->d_disp_lr;
+        q.w = h->w;
+        q.h = h->h;
+        q.median = h->p.median ? 1 : 0;
+        q.min_disp = h->p.sgm.min_disparity;
+        q.out_disp = out.disparity;
+        q.out_conf = out.confidence;
+        q.out_u16 = out.disparity_u16;
+        q.out_depth = h->have_points ? out.depth : nullptr;
+        q.f = h->geom.f;
+        q.baseline = h->geom.baseline;
+        q.cx_offset = h->geom.cx_offset;
+        q.min_depth = h->min_depth;
+        q.max_depth = h->max_depth;
+        dim3 b(32, 8), g((h->w + 31) / 32, (h->h + 7) / 8);
+        dsk::k_post<<<g, b, 0, st>>>(q);
+        ++g_launches;
+    }
+    marks.mark(5);
+    DS_CUDA(cudaGetLastError());
+}
+
+ds_outputs internal_outputs(ds_handle* h) {
+    ds_outputs o{};
+    o.disparity = h->d_out_disp;
+    o.confidence = h->d_out_conf;
+    o.disparity_u16 = h->d_out_u16;
+    o.depth = h->d_out_depth;
+    return o;
+}
+
+int run_host(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t stride, const ds_outputs* out, bool raw) {
+    const double t0 = now_ms();
+    const int iw = raw ? h->raw_w : h->w, ih = raw ? h->raw_h : h->h;
+    if (!left || !right) return h->fail(DS_INVALID_ARGUMENT, "null image");
+    if (stride < iw) return h->fail(DS_INVALID_ARGUMENT, "stride smaller than the image width");
+    if (out && out->depth && !h->have_points) return h->fail(DS_INVALID_ARGUMENT, "set_point_params() not called");
+    uint8_t* dst[2] = {raw ? h->d_raw[0] : h->d_rect[0], raw ? h->d_raw[1] : h->d_rect[1]};
+    const uint8_t* src[2] = {left, right};
+    for (int s = 0; s < 2; ++s)
+        DS_CUDA(cudaMemcpy2DAsync(dst[s], iw, src[s], stride, iw, ih, cudaMemcpyHostToDevice, h->stream));
+    DS_CUDA(cudaEventRecord(h->ev0, h->stream));
+    enqueue_frame(h, dst[0], dst[1], raw, internal_outputs(h), h->stream);
+    DS_CUDA(cudaEventRecord(h->ev1, h->stream));
+    const size_t n = static_cast<size_t>(h->w) * h->h;
+    if (out) {
+        if (out->disparity) DS_CUDA(cudaMemcpyAsync(out->disparity, h->d_out_disp, n * 4, cudaMemcpyDeviceToHost, h->stream));
+        if (out->confidence) DS_CUDA(cudaMemcpyAsync(out->confidence, h->d_out_conf, n * 4, cudaMemcpyDeviceToHost, h->stream));
+        if (out->disparity_u16) DS_CUDA(cudaMemcpyAsync(out->disparity_u16, h->d_out_u16, n * 2, cudaMemcpyDeviceToHost, h->stream));
+        if (out->depth) DS_CUDA(cudaMemcpyAsync(out->depth, h->d_out_depth, n * 4, cudaMemcpyDeviceToHost, h->stream));
+        if (out->rect_left) DS_CUDA(cudaMemcpyAsync(out->rect_left, h->d_rect[0], n, cudaMemcpyDeviceToHost, h->stream));
+        if (out->rect_right) DS_CUDA(cudaMemcpyAsync(out->rect_right, h->d_rect[1], n, cudaMemcpyDeviceToHost, h->stream));
+    }
+    DS_CUDA(cudaStreamSynchronize(h->stream));
+    float ms = 0.0f;
+    DS_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    h->timings.gpu_ms = ms;
+    h->timings.speckle_ms = 0.0;
+    h->timings.total_ms = now_ms() - t0;
+    return DS_OK;
+}
+
+template <typename F>
+int guarded(ds_handle* h, F&& f) {
+    try {
+        return f();
+    } catch (const CudaFailure& e) {
+        std::string m = std::string("CUDA stereo failed: ") + e.what + ": " + cudaGetErrorString(e.err);
+        if (h) h->err = m;
+        g_error = m;
+        return DS_IO;
+    } catch (const std::bad_alloc&) {
+        if (h) h->err = "host allocation failed";
+        g_error = "host allocation failed";
+        return DS_IO;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+DS_API void ds_default_params(ds_stereo_params* p) {
+    if (!p) return;
+    *p = ds_stereo_params{};
+    p->pyramid_levels = 0;
+    p->sgm.min_disparity = 0;
+    p->sgm.num_disparities = 64;
+    p->sgm.census_radius_x = 2;
+    p->sgm.census_radius_y = 2;
+    p->sgm.p1 = 8;
+    p->sgm.p2 = 96;
+    p->sgm.adaptive_p2 = 1;
+    p->sgm.eight_paths = 0;
+    p->sgm.slant_steps = 1;
+    p->sgm.uniqueness = 0.9f;
+    p->sgm.lr_max_diff = 1;
+    p->subpixel = 1;
+    p->median = 1;
+}
+
+DS_API const char* ds_last_global_error(void) { return g_error.c_str(); }
+
+DS_API int ds_create(const ds_stereo_params* params, int width, int height, ds_handle** out) {
+    if (!params || !out) {
+        g_error = "null argument";
+        return DS_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    std::string msg;
+    if (const int rc = validate(*params, width, height, msg); rc != DS_OK) {
+        g_error = msg;
+        return rc;
+    }
+    auto* h = new (std::nothrow) ds_handle();
+    if (!h) {
+        g_error = "host allocation failed";
+        return DS_IO;
+    }
+    const int rc = guarded(h, [&]() -> int {
+        h->p = *params;
+        h->w = width;
+        h->h = height;
+        h->nd = params->sgm.num_disparities;
+        h->vpl = round_vpl(h->nd);
+        h->dp = 32 * h->vpl;
+        h->ndirs = params->sgm.eight_paths ? 8 : 4;
+        const int window = (2 * params->sgm.census_radius_x + 1) * (2 * params->sgm.census_radius_y + 1);
+        h->census64 = window - 1 > 32;
+        // Path values are at most window + P2 (the recurrence never lets best exceed min(prev) + P2).
+        h->wide = params->wide_costs || window + params->sgm.p2 > 255;
+        DS_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        DS_CUDA(cudaEventCreate(&h->ev0));
+        DS_CUDA(cudaEventCreate(&h->ev1));
+        const size_t n = static_cast<size_t>(width) * height;
+        h->d_rect[0] = h->alloc<uint8_t>(n);
+        h->d_rect[1] = h->alloc<uint8_t>(n);
+        const size_t cw = h->census64 ? 8 : 4;
+        h->d_census[0] = h->alloc<uint8_t>(n * cw);
+        h->d_census[1] = h->alloc<uint8_t>(n * cw);
+        h->dir_stride = n * static_cast<size_t>(h->dp);
+        h->d_values = h->alloc<uint8_t>(h->dir_stride * h->ndirs * (h->wide ? 2 : 1));
+        h->d_disp_lr = h->alloc<float>(n);
+        h->d_out_disp = h->alloc<float>(n);
+        h->d_out_conf = h->alloc<float>(n);
+        h->d_out_u16 = h->alloc<uint16_t>(n);
+        h->d_out_depth = h->alloc<float>(n);
+        return DS_OK;
+    });
+    if (rc != DS_OK) {
+        g_error = h->err;
+        release(h);
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return DS_OK;
+}
+
+DS_API void ds_destroy(ds_handle* h) {
+    if (!h) return;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    release(h);
+    delete h;
+}
+
+DS_API int ds_set_rectification(ds_handle* h, const float* lx, const float* ly, const float* rx, const float* ry, int map_w,
+                                int map_h, int raw_w, int raw_h) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    if (!lx || !ly || !rx || !ry) return h->fail(DS_INVALID_ARGUMENT, "null remap table");
+    const bool same = map_w == h->w && map_h == h->h;
+    const bool twice = map_w == 2 * h->w && map_h == 2 * h->h;
+    if (!same && !twice) return h->fail(DS_INVALID_ARGUMENT, "remap resolution must be the stereo resolution or twice it");
+    if (raw_w < 2 || raw_h < 2 || raw_w > 16384 || raw_h > 16384) return h->fail(DS_INVALID_ARGUMENT, "raw size out of range");
+    return guarded(h, [&]() -> int {
+        const size_t n = static_cast<size_t>(map_w) * map_h;
+        if (h->map_w != map_w || h->map_h != map_h) {
+            for (auto*& p : h->d_map) {
+                if (p) {
+                    cudaFree(p);
+                    h->bytes -= static_cast<size_t>(h->map_w) * h->map_h * 4;
+                    p = nullptr;
+                }
+            }
+            for (auto*& p : h->d_map) p = h->alloc<float>(n);
+        }
+        if (h->raw_w != raw_w || h->raw_h != raw_h) {
+            for (auto*& p : h->d_raw) {
+                if (p) {
+                    cudaFree(p);
+                    h->bytes -= static_cast<size_t>(h->raw_w) * h->raw_h;
+                    p = nullptr;
+                }
+            }
+            for (auto*& p : h->d_raw) p = h->alloc<uint8_t>(static_cast<size_t>(raw_w) * raw_h);
+        }
+        const float* src[4] = {lx, ly, rx, ry};
+        for (int i = 0; i < 4; ++i) DS_CUDA(cudaMemcpyAsync(h->d_map[i], src[i], n * 4, cudaMemcpyHostToDevice, h->stream));
+        DS_CUDA(cudaStreamSynchronize(h->stream));
+        h->map_w = map_w;
+        h->map_h = map_h;
+        h->raw_w = raw_w;
+        h->raw_h = raw_h;
+        h->have_rect = true;
+        return DS_OK;
+    });
+}
+
+DS_API int ds_set_point_params(ds_handle* h, const ds_geometry* g, float min_depth, float max_depth, float max_jump) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    if (!g) return h->fail(DS_INVALID_ARGUMENT, "null geometry");
+    h->geom = *g;
+    h->min_depth = min_depth;
+    h->max_depth = max_depth;
+    h->max_jump = max_jump;
+    h->have_points = true;
+    return DS_OK;
+}
+
+DS_API int ds_compute(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t stride, const ds_outputs* out) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    return guarded(h, [&] { return run_host(h, left, right, stride, out, false); });
+}
+
+DS_API int ds_compute_raw(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t stride, const ds_outputs* out) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    if (!h->have_rect) return h->fail(DS_INVALID_ARGUMENT, "set_rectification() not called");
+    return guarded(h, [&] { return run_host(h, left, right, stride, out, true); });
+}
+
+static int run_device(ds_handle* h, const uint8_t* left, const uint8_t* right, const ds_outputs* out, void* stream, bool raw) {
+    if (!left || !right) return h->fail(DS_INVALID_ARGUMENT, "null image");
+    if (raw && !h->have_rect) return h->fail(DS_INVALID_ARGUMENT, "set_rectification() not called");
+    if (out && out->depth && !h->have_points) return h->fail(DS_INVALID_ARGUMENT, "set_point_params() not called");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+    return guarded(h, [&]() -> int {
+        ds_outputs o = out ? *out : ds_outputs{};
+        enqueue_frame(h, left, right, raw, o, st);
+        const size_t n = static_cast<size_t>(h->w) * h->h;
+        if (raw && o.rect_left) DS_CUDA(cudaMemcpyAsync(o.rect_left, h->d_rect[0], n, cudaMemcpyDeviceToDevice, st));
+        if (raw && o.rect_right) DS_CUDA(cudaMemcpyAsync(o.rect_right, h->d_rect[1], n, cudaMemcpyDeviceToDevice, st));
+        return DS_OK;
+    });
+}
+
+DS_API int ds_compute_device(ds_handle* h, const uint8_t* left, const uint8_t* right, const ds_outputs* out, void* stream) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    return run_device(h, left, right, out, stream, false);
+}
+
+DS_API int ds_compute_raw_device(ds_handle* h, const uint8_t* left, const uint8_t* right, const ds_outputs* out, void* stream) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    return run_device(h, left, right, out, stream, true);
+}
+
+DS_API int ds_last_timings(const ds_handle* h, ds_timings* out) {
+    if (!h || !out) return DS_INVALID_ARGUMENT;
+    *out = h->timings;
+    return DS_OK;
+}
+
+DS_API const char* ds_last_error(const ds_handle* h) { return h ? h->err.c_str() : g_error.c_str(); }
+
+DS_API int ds_debug_read(ds_handle* h, uint64_t* census_left, uint64_t* census_right, uint16_t* path_sums) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    return guarded(h, [&]() -> int {
+        const size_t n = static_cast<size_t>(h->w) * h->h;
+        DS_CUDA(cudaStreamSynchronize(h->stream));
+        uint64_t* dst[2] = {census_left, census_right};
+        for (int s = 0; s < 2; ++s) {
+            if (!dst[s]) continue;
+            if (h->census64) {
+                DS_CUDA(cudaMemcpy(dst[s], h->d_census[s], n * 8, cudaMemcpyDeviceToHost));
+            } else {
+                std::vector<uint32_t> tmp(n);
+                DS_CUDA(cudaMemcpy(tmp.data(), h->d_census[s], n * 4, cudaMemcpyDeviceToHost));
+                for (size_t i = 0; i < n; ++i) dst[s][i] = tmp[i];
+            }
+        }
+        if (path_sums) {
+            const size_t m = n * h->nd;
+            uint16_t* d = nullptr;
+            DS_CUDA(cudaMalloc(&d, m * 2));
+            dsk::SumArgs a{h->d_values, h->dir_stride, h->ndirs, h->w, h->h, h->nd, h->dp, d};
+            if (h->wide) dsk::k_debug_sums<uint16_t><<<1024, 256, 0, h->stream>>>(a);
+            else dsk::k_debug_sums<uint8_t><<<1024, 256, 0, h->stream>>>(a);
+            cudaError_t e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaMemcpyAsync(path_sums, d, m * 2, cudaMemcpyDeviceToHost, h->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+            cudaFree(d);
+            if (e != cudaSuccess) throw CudaFailure{e, "debug sums"};
+        }
+        return DS_OK;
+    });
+}
+
+DS_API size_t ds_device_bytes(const ds_handle* h) { return h ? h->bytes : 0; }
+
+DS_API int ds_profile_enable(ds_handle* h, int on) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    return guarded(h, [&]() -> int {
+        if (on && h->prof_events.empty()) {
+            h->prof_events.resize(static_cast<size_t>(kProfileRing) * (DS_STAGES + 1));
+            for (auto& e : h->prof_events) DS_CUDA(cudaEventCreate(&e));
+        }
+        h->profile = on != 0;
+        return DS_OK;
+    });
+}
+
+DS_API int ds_profile_collect(ds_handle* h, double* stage_ms, int max_frames, int* frames) {
+    if (!h || !frames) return DS_INVALID_ARGUMENT;
+    return guarded(h, [&]() -> int {
+        int n = 0;
+        while (h->prof_pending > 0) {
+            cudaEvent_t* ev = &h->prof_events[static_cast<size_t>(h->prof_head) * (DS_STAGES + 1)];
+            DS_CUDA(cudaEventSynchronize(ev[DS_STAGES]));
+            if (n < max_frames && stage_ms) {
+                for (int i = 0; i < DS_STAGES; ++i) {
+                    float ms = 0.0f;
+                    DS_CUDA(cudaEventElapsedTime(&ms, ev[i], ev[i + 1]));
+                    stage_ms[static_cast<size_t>(n) * DS_STAGES + i] = ms;
+                }
+                ++n;
+            }
+            h->prof_head = (h->prof_head + 1) % kProfileRing;
+            --h->prof_pending;
+        }
+        *frames = n;
+        return DS_OK;
+    });
+}
+
+DS_API uint64_t ds_kernel_launches(void) { return g_launches.load(); }
+
+}  // extern "C"

@@ -1,0 +1,309 @@
+"""Host-side mirror of the reference's stereo-matcher interface, over the C ABI (include/depth_cuda.h).
+
+Names, argument meaning and error behaviour follow:
+  depth::SgmParams / StereoParams / StereoResult   libs/depth/include/einstar/depth/stereo.hpp:26-93
+  depth::RectifiedGeometry                         libs/depth/include/einstar/depth/point_image.hpp:12-26
+  calib::RemapTable                                libs/calib/include/einstar/calib/rectify.hpp:40-44
+  depth_metal::MetalStereo, StereoTimings          libs/depth_metal/include/einstar/depth_metal/metal_stereo.hpp:61-107
+  einstar::Errc / Result                           libs/core/include/einstar/core/error.hpp:8-33
+A Result error becomes a StereoError carrying the Errc and the message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+
+INVALID_DISPARITY = np.float32(-1.0e9)  # depth::kInvalidDisparity
+
+
+def valid_disparity(d):
+    """depth::valid_disparity (stereo.hpp:24)."""
+    return d > -1.0e8
+
+
+class Errc(enum.IntEnum):
+    ok = 0
+    not_found = 1
+    io = 2
+    timeout = 3
+    protocol = 4
+    invalid_argument = 5
+    blocked = 6
+    unsupported = 7
+    busy = 8
+    disconnected = 9
+
+
+class StereoError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        self.code = Errc(code)
+        self.message = message
+        super().__init__(f"{self.code.name}: {message}")
+
+
+@dataclass
+class SgmParams:
+    min_disparity: int = 0
+    num_disparities: int = 64
+    census_radius_x: int = 2
+    census_radius_y: int = 2
+    p1: int = 8
+    p2: int = 96
+    adaptive_p2: bool = True
+    eight_paths: bool = False
+    slant_steps: bool = True
+    uniqueness: float = 0.9
+    lr_max_diff: int = 1
+
+
+@dataclass
+class StereoParams:
+    """depth::StereoParams reduced to the hot path (pyramid 0, subpixel, median). The later stages keep
+    their switches; asking for them raises StereoError(unsupported), as the C ABI returns."""
+    pyramid_levels: int = 0
+    sgm: SgmParams = field(default_factory=SgmParams)
+    subpixel: bool = True
+    median: bool = True
+    detail_enabled: bool = False
+    filter_occlusion: bool = False
+    filter_spikes: bool = False
+    speckle_max_region_size: int = 0
+    wide_costs: bool = False
+
+    def c(self) -> N.StereoParamsC:
+        s = self.sgm
+        return N.StereoParamsC(
+            self.pyramid_levels,
+            N.SgmParamsC(s.min_disparity, s.num_disparities, s.census_radius_x, s.census_radius_y, s.p1, s.p2,
+                         int(bool(s.adaptive_p2)), int(bool(s.eight_paths)), int(bool(s.slant_steps)),
+                         float(s.uniqueness), s.lr_max_diff),
+            int(bool(self.subpixel)), int(bool(self.median)), int(bool(self.detail_enabled)),
+            int(bool(self.filter_occlusion)), int(bool(self.filter_spikes)), int(self.speckle_max_region_size),
+            int(bool(self.wide_costs)))
+
+
+@dataclass
+class RectifiedGeometry:
+    f: float = 0.0
+    cx: float = 0.0
+    cy: float = 0.0
+    baseline: float = 0.0
+    cx_offset: float = 0.0
+
+    def depth_from_disparity(self, d):
+        return self.f * self.baseline / (d + self.cx_offset)
+
+    def disparity_from_depth(self, z):
+        return self.f * self.baseline / z - self.cx_offset
+
+
+@dataclass
+class RemapTable:
+    """calib::RemapTable: for each rectified pixel the source pixel in the raw image (float32)."""
+    map_x: np.ndarray
+    map_y: np.ndarray
+
+    @property
+    def width(self) -> int:
+        return int(self.map_x.shape[1])
+
+    @property
+    def height(self) -> int:
+        return int(self.map_x.shape[0])
+
+
+@dataclass
+class StereoTimings:
+    gpu_ms: float = 0.0
+    speckle_ms: float = 0.0
+    total_ms: float = 0.0
+
+
+@dataclass
+class StereoResult:
+    """depth::StereoResult (disparity, confidence) plus this library's u16 disparity and depth."""
+    disparity: np.ndarray
+    confidence: np.ndarray
+    disparity_u16: np.ndarray | None = None
+    depth: np.ndarray | None = None
+    rect_left: np.ndarray | None = None
+    rect_right: np.ndarray | None = None
+
+
+def _ptr(a) -> int | None:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a.data_ptr())  # a device tensor (plumbing only: just its address crosses the ABI)
+
+
+def _check_u8(img: np.ndarray, w: int, h: int, what: str) -> np.ndarray:
+    img = np.asarray(img)
+    if img.dtype != np.uint8 or img.ndim != 2:
+        raise StereoError(Errc.invalid_argument, f"{what}: expected a 2-D uint8 image")
+    if img.shape != (h, w):
+        raise StereoError(Errc.invalid_argument, f"{what}: image size does not match the configured size")
+    if img.strides[1] != 1:
+        img = np.ascontiguousarray(img)
+    return img
+
+
+class CudaStereo:
+    """Drop-in for depth_metal::MetalStereo on the hot path (create / set_rectification / compute /
+    compute_raw / set_point_params / last_timings)."""
+
+    def __init__(self, handle: int, params: StereoParams, width: int, height: int):
+        self._h = C.c_void_p(handle)
+        self.params = params
+        self.width = width
+        self.height = height
+        self.raw_size: tuple[int, int] | None = None
+        self.geometry: RectifiedGeometry | None = None
+
+    # --- life cycle ---------------------------------------------------------------------------------
+    @classmethod
+    def create(cls, params: StereoParams, width: int, height: int) -> "CudaStereo":
+        """MetalStereo::create (metal_stereo.cpp:108-201): validates and allocates device buffers."""
+        L = N.lib()
+        h = C.c_void_p()
+        rc = L.ds_create(C.byref(params.c()), int(width), int(height), C.byref(h))
+        if rc != 0:
+            raise StereoError(rc, L.ds_last_global_error().decode())
+        return cls(h.value, params, int(width), int(height))
+
+    def close(self) -> None:
+        if self._h:
+            N.lib().ds_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            raise StereoError(rc, N.lib().ds_last_error(self._h).decode())
+
+    # --- configuration ------------------------------------------------------------------------------
+    def set_rectification(self, left: RemapTable, right: RemapTable, raw_width: int, raw_height: int) -> None:
+        """MetalStereo::set_rectification (metal_stereo.cpp:203-231): tables resident on the device."""
+        if (left.width, left.height) != (right.width, right.height):
+            raise StereoError(Errc.invalid_argument, "left and right remap tables differ in size")
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (left.map_x, left.map_y, right.map_x, right.map_y)]
+        self._check(N.lib().ds_set_rectification(self._h, *[a.ctypes.data for a in arrs], left.width, left.height,
+                                                 int(raw_width), int(raw_height)))
+        self.raw_size = (int(raw_width), int(raw_height))
+
+    def set_point_params(self, geometry: RectifiedGeometry, min_depth_mm: float = 150.0, max_depth_mm: float = 700.0,
+                         max_depth_jump_mm: float = 4.0) -> None:
+        """MetalStereo::set_point_params (metal_stereo.cpp:243-249)."""
+        g = N.GeometryC(geometry.f, geometry.cx, geometry.cy, geometry.baseline, geometry.cx_offset)
+        self._check(N.lib().ds_set_point_params(self._h, C.byref(g), float(min_depth_mm), float(max_depth_mm),
+                                                float(max_depth_jump_mm)))
+        self.geometry = geometry
+
+    # --- per frame ----------------------------------------------------------------------------------
+    def _outputs(self, rect: bool):
+        n = (self.height, self.width)
+        res = StereoResult(np.empty(n, np.float32), np.empty(n, np.float32), np.empty(n, np.uint16),
+                           np.empty(n, np.float32) if self.geometry is not None else None,
+                           np.empty(n, np.uint8) if rect else None, np.empty(n, np.uint8) if rect else None)
+        o = N.OutputsC(_ptr(res.disparity), _ptr(res.confidence), _ptr(res.disparity_u16), _ptr(res.depth),
+                       _ptr(res.rect_left), _ptr(res.rect_right))
+        return res, o
+
+    @staticmethod
+    def _outputs_of(res: StereoResult):
+        return N.OutputsC(_ptr(res.disparity), _ptr(res.confidence), _ptr(res.disparity_u16), _ptr(res.depth),
+                          _ptr(res.rect_left), _ptr(res.rect_right))
+
+    def compute(self, left: np.ndarray, right: np.ndarray, out: StereoResult | None = None) -> StereoResult:
+        """MetalStereo::compute (metal_stereo.cpp:233-241) on an already rectified pair. `out` may hold
+        preallocated host arrays (None entries are not produced)."""
+        left = _check_u8(left, self.width, self.height, "left")
+        right = _check_u8(right, self.width, self.height, "right")
+        if left.strides[0] != right.strides[0]:
+            left, right = np.ascontiguousarray(left), np.ascontiguousarray(right)
+        res, o = (out, self._outputs_of(out)) if out is not None else self._outputs(False)
+        self._check(N.lib().ds_compute(self._h, left.ctypes.data, right.ctypes.data, left.strides[0], C.byref(o)))
+        return res
+
+    def compute_raw(self, raw_left: np.ndarray, raw_right: np.ndarray, rectified: bool = False,
+                    out: StereoResult | None = None) -> StereoResult:
+        """MetalStereo::compute_raw (metal_stereo.cpp:340-349): rectify on the device, then stereo. With
+        `rectified`, the rectified pair is returned too (the rect_left / rect_right out-parameters).
+        `out` may hold preallocated host arrays (None entries are not produced)."""
+        if self.raw_size is None:
+            raise StereoError(Errc.invalid_argument, "set_rectification() not called")
+        rw, rh = self.raw_size
+        raw_left = _check_u8(raw_left, rw, rh, "raw left")
+        raw_right = _check_u8(raw_right, rw, rh, "raw right")
+        if raw_left.strides[0] != raw_right.strides[0]:
+            raw_left, raw_right = np.ascontiguousarray(raw_left), np.ascontiguousarray(raw_right)
+        res, o = (out, self._outputs_of(out)) if out is not None else self._outputs(rectified)
+        self._check(N.lib().ds_compute_raw(self._h, raw_left.ctypes.data, raw_right.ctypes.data, raw_left.strides[0],
+                                           C.byref(o)))
+        return res
+
+    def compute_device(self, left, right, outputs: dict, stream=None, raw: bool = False) -> None:
+        """Device-resident frame: `left`/`right` and every tensor in `outputs` (keys of ds_outputs:
+        disparity, confidence, disparity_u16, depth, rect_left, rect_right) are device buffers; enqueued on
+        `stream` (a torch.cuda.Stream or raw cudaStream_t; None = the handle's stream), not waited for."""
+        o = N.OutputsC(*[_ptr(outputs.get(k)) for k in ("disparity", "confidence", "disparity_u16", "depth",
+                                                        "rect_left", "rect_right")])
+        s = None if stream is None else (stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        fn = N.lib().ds_compute_raw_device if raw else N.lib().ds_compute_device
+        self._check(fn(self._h, _ptr(left), _ptr(right), C.byref(o), s))
+
+    def last_timings(self) -> StereoTimings:
+        t = N.TimingsC()
+        self._check(N.lib().ds_last_timings(self._h, C.byref(t)))
+        return StereoTimings(t.gpu_ms, t.speckle_ms, t.total_ms)
+
+    # --- introspection ------------------------------------------------------------------------------
+    def debug_read(self, census=True, sums=True):
+        """Census words (u64) and summed path values (u16 [y][x][d]) of the last frame."""
+        h, w, nd = self.height, self.width, self.params.sgm.num_disparities
+        cl = np.empty((h, w), np.uint64) if census else None
+        cr = np.empty((h, w), np.uint64) if census else None
+        s = np.empty((h, w, nd), np.uint16) if sums else None
+        self._check(N.lib().ds_debug_read(self._h, _ptr(cl), _ptr(cr), _ptr(s)))
+        return cl, cr, s
+
+    @property
+    def device_bytes(self) -> int:
+        return int(N.lib().ds_device_bytes(self._h))
+
+    def profile(self, on: bool = True) -> None:
+        """Per-stage CUDA events for every frame (stages: rectify, census, paths, wta+lr, median+outputs)."""
+        self._check(N.lib().ds_profile_enable(self._h, int(bool(on))))
+
+    def profile_collect(self, max_frames: int = 4096) -> np.ndarray:
+        """Waits for the profiled frames since the last call; rows of per-stage milliseconds."""
+        buf = np.zeros((max_frames, STAGES), np.float64)
+        n = C.c_int()
+        self._check(N.lib().ds_profile_collect(self._h, buf.ctypes.data, max_frames, C.byref(n)))
+        return buf[:n.value].copy()
+
+
+STAGES = 5
+STAGE_NAMES = ("rectify", "census", "paths", "wta_lr", "median_out")
+
+
+def kernel_launches() -> int:
+    """Kernels the library has launched since it was loaded."""
+    return int(N.lib().ds_kernel_launches())

@@ -1,0 +1,229 @@
+"""numpy front end of the test oracle (ctypes over oracle/_bin/liboracle.so and oracle/_ref/libref_stereo.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, the smoke check and the bench's CPU-baseline leg, as
+the checker or the timed CPU arm. The product package never imports it.
+
+Two implementations of the same functions:
+  Port(): this repository's C restatement (oracle/sgm_oracle.c), always buildable with gcc.
+  Ref():  the reference's own libs/depth/src/stereo.cpp compiled unmodified (oracle/_ref), for
+          census, sgm_disparity and median3; remap and depth (whose reference files need Eigen) come
+          from the port in both.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "_bin", "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libref_stereo.so")
+
+INVALID = np.float32(-1.0e9)
+NO_MATCH = np.int32(-(2**31))
+
+
+class _Sgm(C.Structure):
+    _fields_ = [
+        ("min_disparity", C.c_int), ("num_disparities", C.c_int),
+        ("census_radius_x", C.c_int), ("census_radius_y", C.c_int),
+        ("p1", C.c_int), ("p2", C.c_int), ("adaptive_p2", C.c_int),
+        ("eight_paths", C.c_int), ("slant_steps", C.c_int),
+        ("uniqueness", C.c_float), ("lr_max_diff", C.c_int),
+    ]
+
+
+@dataclass
+class OracleSgm:
+    """Fields of depth::SgmParams (libs/depth/include/einstar/depth/stereo.hpp:26-40), same defaults."""
+    min_disparity: int = 0
+    num_disparities: int = 64
+    census_radius_x: int = 2
+    census_radius_y: int = 2
+    p1: int = 8
+    p2: int = 96
+    adaptive_p2: bool = True
+    eight_paths: bool = False
+    slant_steps: bool = True
+    uniqueness: float = 0.9
+    lr_max_diff: int = 1
+
+    def c(self) -> _Sgm:
+        return _Sgm(self.min_disparity, self.num_disparities, self.census_radius_x, self.census_radius_y,
+                    self.p1, self.p2, int(bool(self.adaptive_p2)), int(bool(self.eight_paths)),
+                    int(bool(self.slant_steps)), float(self.uniqueness), self.lr_max_diff)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _u8(a) -> np.ndarray:
+    a = np.ascontiguousarray(a)
+    assert a.dtype == np.uint8 and a.ndim == 2
+    return a
+
+
+def build(ref: str | None = None) -> None:
+    """Builds the port (and, when the reference tree is present, oracle/_ref) with make."""
+    import subprocess
+    cmd = ["make", "-s", "-C", HERE, "all"]
+    if ref:
+        cmd.append(f"REF={ref}")
+    subprocess.run(cmd, check=True)
+
+
+class Port:
+    """The C restatement (oracle/sgm_oracle.c)."""
+
+    def __init__(self, path: str = PORT_SO):
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        self.lib = L
+        vp, i, f, d = C.c_void_p, C.c_int, C.c_float, C.c_double
+        L.orc_census.argtypes = [vp, i, i, i, i, vp]
+        L.orc_cost_volume.argtypes = [vp, vp, i, i, C.POINTER(_Sgm), vp]
+        L.orc_aggregate.argtypes = [vp, vp, i, i, C.POINTER(_Sgm), vp]
+        L.orc_wta.argtypes = [vp, i, i, C.POINTER(_Sgm), i, vp, vp]
+        L.orc_lr_check.argtypes = [vp, vp, i, i, i]
+        L.orc_sgm_disparity.argtypes = [vp, vp, i, i, C.POINTER(_Sgm), i, vp]
+        L.orc_sgm_disparity.restype = i
+        L.orc_median3.argtypes = [vp, i, i, vp]
+        L.orc_remap.argtypes = [vp, i, i, vp, vp, i, i, vp]
+        L.orc_depth.argtypes = [vp, i, i, d, d, d, f, f, vp]
+        L.orc_encode_u16.argtypes = [vp, C.c_long, i, vp]
+
+    def census(self, img, rx=2, ry=2) -> np.ndarray:
+        img = _u8(img)
+        h, w = img.shape
+        out = np.empty((h, w), np.uint64)
+        self.lib.orc_census(_p(img), w, h, rx, ry, _p(out))
+        return out
+
+    def cost_volume(self, cl, cr, p: OracleSgm) -> np.ndarray:
+        h, w = cl.shape
+        out = np.empty((h, w, p.num_disparities), np.uint16)
+        self.lib.orc_cost_volume(_p(np.ascontiguousarray(cl)), _p(np.ascontiguousarray(cr)), w, h, C.byref(p.c()), _p(out))
+        return out
+
+    def aggregate(self, cost, guide, p: OracleSgm) -> np.ndarray:
+        h, w, nd = cost.shape
+        out = np.empty_like(cost)
+        self.lib.orc_aggregate(_p(np.ascontiguousarray(cost)), _p(_u8(guide)), w, h, C.byref(p.c()), _p(out))
+        return out
+
+    def wta(self, sums, p: OracleSgm, subpixel=True):
+        h, w, nd = sums.shape
+        disp = np.empty((h, w), np.float32)
+        rd = np.empty((h, w), np.int32)
+        self.lib.orc_wta(_p(np.ascontiguousarray(sums)), w, h, C.byref(p.c()), int(subpixel), _p(disp), _p(rd))
+        return disp, rd
+
+    def lr_check(self, disp, rd, lr_max_diff=1) -> np.ndarray:
+        d = np.array(disp, np.float32, copy=True)
+        h, w = d.shape
+        self.lib.orc_lr_check(_p(d), _p(np.ascontiguousarray(rd, np.int32)), w, h, lr_max_diff)
+        return d
+
+    def sgm_disparity(self, left, right, p: OracleSgm, subpixel=True) -> np.ndarray:
+        left, right = _u8(left), _u8(right)
+        h, w = left.shape
+        out = np.empty((h, w), np.float32)
+        if self.lib.orc_sgm_disparity(_p(left), _p(right), w, h, C.byref(p.c()), int(subpixel), _p(out)) != 0:
+            raise MemoryError("oracle allocation failed")
+        return out
+
+    def median3(self, disp) -> np.ndarray:
+        d = np.ascontiguousarray(disp, np.float32)
+        h, w = d.shape
+        out = np.empty_like(d)
+        self.lib.orc_median3(_p(d), w, h, _p(out))
+        return out
+
+    def remap(self, src, map_x, map_y) -> np.ndarray:
+        src = _u8(src)
+        mx = np.ascontiguousarray(map_x, np.float32)
+        my = np.ascontiguousarray(map_y, np.float32)
+        h, w = mx.shape
+        out = np.empty((h, w), np.uint8)
+        self.lib.orc_remap(_p(src), src.shape[1], src.shape[0], _p(mx), _p(my), w, h, _p(out))
+        return out
+
+    def depth(self, disp, f, baseline, cx_offset=0.0, min_depth=150.0, max_depth=700.0) -> np.ndarray:
+        d = np.ascontiguousarray(disp, np.float32)
+        h, w = d.shape
+        out = np.empty_like(d)
+        self.lib.orc_depth(_p(d), w, h, float(f), float(baseline), float(cx_offset), float(min_depth), float(max_depth), _p(out))
+        return out
+
+    def encode_u16(self, disp, min_disparity) -> np.ndarray:
+        d = np.ascontiguousarray(disp, np.float32)
+        out = np.empty(d.shape, np.uint16)
+        self.lib.orc_encode_u16(_p(d), d.size, int(min_disparity), _p(out))
+        return out
+
+    def pipeline(self, left, right, p: OracleSgm, *, subpixel=True, median=True, geometry=None,
+                 min_depth=150.0, max_depth=700.0, maps=None):
+        """The whole hot path: [remap] -> sgm_disparity -> [median3] -> u16 encoding -> depth."""
+        return _pipeline(self, left, right, p, subpixel, median, geometry, min_depth, max_depth, maps)
+
+
+class Ref(Port):
+    """The reference's own stereo.cpp (oracle/_ref) for census / sgm_disparity / median3."""
+
+    def __init__(self, path: str = REF_SO, port_path: str = PORT_SO):
+        super().__init__(port_path)
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (needs the reference tree at build time)")
+        R = C.CDLL(path)
+        self.ref = R
+        vp, i = C.c_void_p, C.c_int
+        R.ref_census.argtypes = [vp, i, i, i, i, vp]
+        R.ref_sgm_disparity.argtypes = [vp, vp, i, i, C.POINTER(_Sgm), i, vp]
+        R.ref_median3.argtypes = [vp, i, i, vp]
+        R.ref_threads.restype = i
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(REF_SO)
+
+    def threads(self) -> int:
+        return int(self.ref.ref_threads())
+
+    def census(self, img, rx=2, ry=2) -> np.ndarray:
+        img = _u8(img)
+        h, w = img.shape
+        out = np.empty((h, w), np.uint64)
+        self.ref.ref_census(_p(img), w, h, rx, ry, _p(out))
+        return out
+
+    def sgm_disparity(self, left, right, p: OracleSgm, subpixel=True) -> np.ndarray:
+        left, right = _u8(left), _u8(right)
+        h, w = left.shape
+        out = np.empty((h, w), np.float32)
+        self.ref.ref_sgm_disparity(_p(left), _p(right), w, h, C.byref(p.c()), int(subpixel), _p(out))
+        return out
+
+    def median3(self, disp) -> np.ndarray:
+        d = np.ascontiguousarray(disp, np.float32)
+        h, w = d.shape
+        out = np.empty_like(d)
+        self.ref.ref_median3(_p(d), w, h, _p(out))
+        return out
+
+
+def _pipeline(o, left, right, p, subpixel, median, geometry, min_depth, max_depth, maps):
+    if maps is not None:
+        (lx, ly), (rx, ry) = maps
+        left, right = o.remap(left, lx, ly), o.remap(right, rx, ry)
+    disp = o.sgm_disparity(left, right, p, subpixel)
+    if median:
+        disp = o.median3(disp)
+    out = {"left": left, "right": right, "disparity": disp, "disparity_u16": o.encode_u16(disp, p.min_disparity)}
+    if geometry is not None:
+        f, baseline, cx_offset = geometry
+        out["depth"] = o.depth(disp, f, baseline, cx_offset, min_depth, max_depth)
+    return out

@@ -1,0 +1,192 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle: bit-exact integer and float stages.
+
+The reference's own GPU-vs-CPU test allows 0.25 px (tests/depth/test_metal_stereo.cpp:120); this path
+is held to bit-identical disparities. Depth is computed in double like the reference and is compared
+bit-for-bit too (the stated tolerance, 1e-4 relative, is asserted as well).
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import mismatch_report, same_bits
+from oracle.oracle import OracleSgm
+
+pytestmark = pytest.mark.gpu
+
+DEPTH_RTOL = 1e-4        # stated tolerance for depth (relative)
+U16_TOL = 1              # 1/64 px: the u16 encoding's step
+
+
+def _stereo(params: OracleSgm, w, h, subpixel=True, median=False, wide=False):
+    from open_source_einstar_b200 import CudaStereo, SgmParams, StereoParams
+    sp = StereoParams(sgm=SgmParams(**params.__dict__), subpixel=subpixel, median=median, wide_costs=wide)
+    return CudaStereo.create(sp, w, h)
+
+
+def test_golden_cases_bit_exact(cuda, golden):
+    for name, c in golden.items():
+        p = OracleSgm(**c["params"])
+        h, w = c["shape"]
+        with _stereo(p, w, h, c["subpixel"], median=False) as s:
+            r = s.compute(c["left"], c["right"])
+            if "disparity" in c:
+                assert same_bits(r.disparity, c["disparity"]), f"{name}: {mismatch_report(r.disparity, c['disparity'])}"
+            else:
+                assert hashlib.sha256(r.disparity.tobytes()).hexdigest() == c["disparity_sha256"], name
+            assert np.array_equal(r.confidence, (r.disparity > -1e8).astype(np.float32))
+            if "census_left" in c:
+                cl, _, _ = s.debug_read(census=True, sums=False)
+                assert same_bits(cl, c["census_left"]), name
+        with _stereo(p, w, h, c["subpixel"], median=True) as s:
+            r = s.compute(c["left"], c["right"])
+            if "median" in c:
+                assert same_bits(r.disparity, c["median"]), f"{name} (median): {mismatch_report(r.disparity, c['median'])}"
+            else:
+                assert hashlib.sha256(r.disparity.tobytes()).hexdigest() == c["median_sha256"], name
+
+
+def test_path_sums_match_oracle(cuda, golden, port):
+    """Stage check: the summed path costs (the reference's u16 `sum` volume) are identical."""
+    for name in ("plane_sphere_160x128", "eight_paths", "census_9x7_wide", "tiny_37x29_d5", "d_not_multiple_of_32_d40"):
+        c = golden[name]
+        p = OracleSgm(**c["params"])
+        h, w = c["shape"]
+        with _stereo(p, w, h) as s:
+            s.compute(c["left"], c["right"])
+            cl, cr, sums = s.debug_read()
+        cost = port.cost_volume(port.census(c["left"], p.census_radius_x, p.census_radius_y),
+                                port.census(c["right"], p.census_radius_x, p.census_radius_y), p)
+        want = port.aggregate(cost, c["left"], p)
+        assert same_bits(sums, want), f"{name}: {mismatch_report(sums, want)}"
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_config1_plane_sphere_full_outputs(cuda, port, seed):
+    """640x512, D=64, default SGM: u16 disparity and f32 depth against the oracle pipeline."""
+    from open_source_einstar_b200 import RectifiedGeometry, synth
+    pair = synth.plane_sphere_pair(seed=seed)
+    p = OracleSgm(min_disparity=pair.min_disparity, num_disparities=pair.num_disparities)
+    want = port.pipeline(pair.left, pair.right, p, median=True, geometry=(pair.f, pair.baseline, 0.0))
+    with _stereo(p, 640, 512, median=True) as s:
+        s.set_point_params(RectifiedGeometry(pair.f, 319.5, 255.5, pair.baseline, 0.0), 150.0, 700.0)
+        r = s.compute(pair.left, pair.right)
+        t = s.last_timings()
+    assert same_bits(r.disparity, want["disparity"]), mismatch_report(r.disparity, want["disparity"])
+    assert np.array_equal(r.disparity_u16, want["disparity_u16"])
+    assert np.abs(r.disparity_u16.astype(int) - want["disparity_u16"].astype(int)).max() <= U16_TOL
+    zw, zg = want["depth"], r.depth
+    assert np.array_equal(zg > 0, zw > 0)
+    nz = zw > 0
+    assert np.all(np.abs(zg[nz] - zw[nz]) <= DEPTH_RTOL * zw[nz])
+    assert same_bits(zg, zw)
+    assert (r.disparity > -1e8).mean() > 0.6
+    assert t.gpu_ms > 0 and t.total_ms >= t.gpu_ms
+
+
+def test_config2_raw_1280x1024_d128(cuda, ref, port):
+    """Raw distorted pair -> GPU remap (bit-exact rectified bytes) -> SGM D=128 -> L-R -> median -> depth."""
+    from open_source_einstar_b200 import CudaStereo, RectifiedGeometry, RemapTable, SgmParams, StereoParams, synth
+    pair = synth.raw_objects_pair(seed=0, device="cuda")
+    (lx, ly), (rx, ry) = pair.maps
+    p = OracleSgm(min_disparity=pair.min_disparity, num_disparities=128)
+    with CudaStereo.create(StereoParams(sgm=SgmParams(**p.__dict__)), 1280, 1024) as s:
+        s.set_rectification(RemapTable(lx, ly), RemapTable(rx, ry), 1280, 1024)
+        s.set_point_params(RectifiedGeometry(pair.f, 0, 0, pair.baseline, 0.0), 150.0, 700.0)
+        r = s.compute_raw(pair.left, pair.right, rectified=True)
+    rl, rr = port.remap(pair.left, lx, ly), port.remap(pair.right, rx, ry)
+    assert np.array_equal(r.rect_left, rl) and np.array_equal(r.rect_right, rr)  # test_metal_stereo.cpp:103
+    d = ref.median3(ref.sgm_disparity(rl, rr, p))
+    assert same_bits(r.disparity, d), mismatch_report(r.disparity, d)
+    z = port.depth(d, pair.f, pair.baseline, 0.0, 150.0, 700.0)
+    assert same_bits(r.depth, z)
+
+
+def test_half_resolution_rectification(cuda, port):
+    """Remap tables at twice the stereo size: remap + 2x2 box average (calib::remap + depth::downsample2)."""
+    from open_source_einstar_b200 import CudaStereo, RemapTable, SgmParams, StereoParams, synth
+    pair = synth.raw_objects_pair(seed=3, width=320, height=256, f=275.0, num_disparities=32, n_objects=8, device="cuda")
+    (lx, ly), (rx, ry) = pair.maps
+    p = OracleSgm(min_disparity=pair.min_disparity // 2, num_disparities=32)
+    with CudaStereo.create(StereoParams(sgm=SgmParams(**p.__dict__)), 160, 128) as s:
+        s.set_rectification(RemapTable(lx, ly), RemapTable(rx, ry), 320, 256)
+        r = s.compute_raw(pair.left, pair.right, rectified=True)
+
+    def down(img):
+        a = img.astype(np.int32)
+        return ((a[0::2, 0::2] + a[0::2, 1::2] + a[1::2, 0::2] + a[1::2, 1::2] + 2) // 4).astype(np.uint8)
+
+    hl, hr = down(port.remap(pair.left, lx, ly)), down(port.remap(pair.right, rx, ry))
+    assert np.array_equal(r.rect_left, hl) and np.array_equal(r.rect_right, hr)
+    assert same_bits(r.disparity, port.median3(port.sgm_disparity(hl, hr, p)))
+
+
+def test_wide_eight_path_d256(cuda, port):
+    """The offline configuration's arithmetic at a small size: 8 paths, D=256, 16-bit path values."""
+    from open_source_einstar_b200 import synth
+    pair = synth.plane_sphere_pair(seed=5, width=320, height=200, f=450.0, num_disparities=256)
+    p = OracleSgm(min_disparity=max(pair.min_disparity - 60, 0), num_disparities=256, eight_paths=True)
+    with _stereo(p, 320, 200, median=True, wide=True) as s:
+        r = s.compute(pair.left, pair.right)
+    want = port.median3(port.sgm_disparity(pair.left, pair.right, p))
+    assert same_bits(r.disparity, want), mismatch_report(r.disparity, want)
+
+
+def test_repeated_frames_bit_identical(cuda, golden):
+    """tests/depth/test_metal_stereo.cpp:157: repeated frames give identical bytes."""
+    c = golden["plane_sphere_160x128"]
+    p = OracleSgm(**c["params"])
+    with _stereo(p, 160, 128, median=True) as s:
+        outs = [s.compute(c["left"], c["right"]) for _ in range(3)]
+    for o in outs[1:]:
+        assert same_bits(o.disparity, outs[0].disparity) and np.array_equal(o.disparity_u16, outs[0].disparity_u16)
+
+
+def test_device_entry_matches_host_entry(cuda, golden):
+    import torch
+    c = golden["plane_sphere_160x128"]
+    p = OracleSgm(**c["params"])
+    with _stereo(p, 160, 128, median=True) as s:
+        host = s.compute(c["left"], c["right"])
+        l = torch.from_numpy(c["left"]).cuda()
+        r = torch.from_numpy(c["right"]).cuda()
+        out = {"disparity": torch.empty((128, 160), dtype=torch.float32, device="cuda"),
+               "disparity_u16": torch.empty((128, 160), dtype=torch.int16, device="cuda")}
+        st = torch.cuda.current_stream()
+        s.compute_device(l, r, out, stream=st)
+        st.synchronize()
+    assert same_bits(out["disparity"].cpu().numpy(), host.disparity)
+    assert np.array_equal(out["disparity_u16"].cpu().numpy().view(np.uint16), host.disparity_u16)
+
+
+def test_strided_host_images(cuda, golden):
+    c = golden["plane_sphere_160x128"]
+    p = OracleSgm(**c["params"])
+    big_l = np.zeros((128, 200), np.uint8)
+    big_r = np.zeros((128, 200), np.uint8)
+    big_l[:, 10:170] = c["left"]
+    big_r[:, 10:170] = c["right"]
+    with _stereo(p, 160, 128) as s:
+        r = s.compute(big_l[:, 10:170], big_r[:, 10:170])
+    assert same_bits(r.disparity, c["disparity"])
+
+
+def test_errors_follow_the_reference(cuda, golden):
+    from open_source_einstar_b200 import Errc, StereoError
+    c = golden["plane_sphere_160x128"]
+    p = OracleSgm(**c["params"])
+    with _stereo(p, 160, 128) as s:
+        with pytest.raises(StereoError) as e:
+            s.compute(c["left"][:100], c["right"][:100])  # metal_stereo.cpp:235-236
+        assert e.value.code == Errc.invalid_argument
+        with pytest.raises(StereoError) as e:
+            s.compute_raw(c["left"], c["right"])  # metal_stereo.cpp:343
+        assert e.value.code == Errc.invalid_argument and "set_rectification" in e.value.message
+        from open_source_einstar_b200 import RemapTable
+        m = np.zeros((100, 100), np.float32)
+        with pytest.raises(StereoError) as e:
+            s.set_rectification(RemapTable(m, m), RemapTable(m, m), 100, 100)  # metal_stereo.cpp:205-206
+        assert e.value.code == Errc.invalid_argument
+        # the handle stays usable after rejected calls
+        r = s.compute(c["left"], c["right"])
+        assert same_bits(r.disparity, c["disparity"])
