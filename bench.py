@@ -62,7 +62,7 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms from warm-up to the end of the e2e run."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -76,7 +76,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -198,6 +198,7 @@ def main():
     ap.add_argument("--frames", type=int, default=8, help="frames per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-budget", type=float, default=150.0, help="seconds of timed reference work at most")
+    ap.add_argument("--kernel-config", default="", help="R,SEG,MATERIALIZE override (default: the library's choice)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -222,10 +223,14 @@ def main():
     s.set_rectification(RemapTable(lx, ly), RemapTable(rx, ry), W, H)
     s.set_point_params(RectifiedGeometry(pairs[0].f, 0, 0, pairs[0].baseline, 0.0), 150.0, 700.0)
 
+    if args.kernel_config:
+        r, seg, mat = (int(v) for v in args.kernel_config.split(","))
+        s.set_kernel_config(r, seg, bool(mat))
     raw = [(torch.from_numpy(p.left).to(dev), torch.from_numpy(p.right).to(dev)) for p in pairs]
     outs = [{"disparity_u16": torch.empty((H, W), dtype=torch.int16, device=dev),
              "depth": torch.empty((H, W), dtype=torch.float32, device=dev)} for _ in range(B)]
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
 
     def step():
         for (l, r), o in zip(raw, outs):
@@ -236,6 +241,7 @@ def main():
             torch.distributed.barrier()
         torch.cuda.synchronize(dev)
 
+    clk = ClockSampler(local).__enter__()
     for _ in range(args.warmup):
         step()
     barrier()
@@ -245,13 +251,12 @@ def main():
     s.profile_collect()
     launches0 = kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        barrier()
-        e0.record(stream)
-        for _ in range(args.steps):
-            step()
-        e1.record(stream)
-        barrier()
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    barrier()
     launches = kernel_launches() - launches0
     ms = e0.elapsed_time(e1)
     stages = s.profile_collect(max_frames=B * args.steps + 8)
@@ -284,6 +289,7 @@ def main():
     if world > 1:
         torch.distributed.all_reduce(e2e_s, op=torch.distributed.ReduceOp.MAX)
     e2e_value = B * e2e_steps * world * PX_D / float(e2e_s.item()) / 1e9
+    clk.__exit__(None, None, None)
 
     # ---- roofline of the dominant kernel --------------------------------------------------------------
     stage_mean = stages.mean(axis=0) if len(stages) else np.zeros(5)
@@ -320,6 +326,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8", "data": "synthetic",
             "config": {"workload": WORKLOAD, "frames_per_step": B, "path": "per-frame launches",
+                       "kernel_config": s.kernel_config(),
                        "l2": "working set per frame (671 MB of path values) far above the 126 MB L2",
                        "parallelism": f"replicas x{world}"},
             "frame_ms": {"p50": float(np.percentile(frame_tot, 50)), "p99": float(np.percentile(frame_tot, 99)),

@@ -134,7 +134,8 @@ DS_API int ds_compute_raw(ds_handle* handle, const uint8_t* raw_left, const uint
 
 /* Device-resident variants (no counterpart in the reference, whose buffers live in unified memory):
  * inputs and outputs are device pointers (tightly packed), the work is enqueued on `stream`
- * (a cudaStream_t; NULL = the handle's own stream) and the call returns without waiting. */
+ * (a cudaStream_t; NULL = the handle's own stream, cudaStreamLegacy for the legacy default stream) and
+ * the call returns without waiting. */
 DS_API int ds_compute_device(ds_handle* handle, const uint8_t* left, const uint8_t* right, const ds_outputs* out,
                              void* stream);
 DS_API int ds_compute_raw_device(ds_handle* handle, const uint8_t* raw_left, const uint8_t* raw_right,
@@ -164,6 +165,26 @@ DS_API int ds_profile_collect(ds_handle* handle, double* stage_ms, int max_frame
 
 /* Number of kernels this library has launched since it was loaded (all handles). */
 DS_API uint64_t ds_kernel_launches(void);
+
+/* Kernel configuration (no counterpart in the reference; the Metal port picks its SIMD variant at
+ * create, metal_stereo.cpp:178-189). A scanline (and a WTA pixel) is run by `lanes_per_line` lanes (16 or
+ * 32) holding 2*regs_per_lane disparities each, so lanes_per_line * 2 * regs_per_lane >= num_disparities.
+ * Supported: 16 lanes with regs 1..4; 32 lanes with regs 1, 2, 3, 4, 6, 8. materialize_costs: write the
+ * matching-cost volume once instead of recomputing costs from the census in every direction. Results are
+ * identical for every configuration; only speed differs (the autotuner chooses). */
+typedef struct ds_kernel_config {
+    int regs_per_lane;
+    int lanes_per_line;
+    int materialize_costs;
+    int path_warps_per_block; /* 1..8 */
+    int wta_threads;          /* multiple of 32, 32..256 */
+    int prefetch_steps;       /* 4 or 8: steps of inputs each scanline keeps in flight */
+    int fused_pairs;          /* 4 paths only: opposite directions as meet-in-the-middle warp pairs, WTA fused
+                               * into the horizontal pair (path_warps_per_block <= 4 per direction) */
+    int horz_warps_per_block; /* fused: warps per direction of the horizontal pair kernel, 1..4 */
+} ds_kernel_config;
+DS_API int ds_set_kernel_config(ds_handle* handle, const ds_kernel_config* config);
+DS_API int ds_get_kernel_config(const ds_handle* handle, ds_kernel_config* config);
 
 #ifdef __cplusplus
 }

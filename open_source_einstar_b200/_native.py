@@ -43,6 +43,12 @@ class OutputsC(C.Structure):
                 ("depth", C.c_void_p), ("rect_left", C.c_void_p), ("rect_right", C.c_void_p)]
 
 
+class KernelConfigC(C.Structure):
+    _fields_ = [("regs_per_lane", C.c_int), ("lanes_per_line", C.c_int), ("materialize_costs", C.c_int),
+                ("path_warps_per_block", C.c_int), ("wta_threads", C.c_int), ("prefetch_steps", C.c_int),
+                ("fused_pairs", C.c_int), ("horz_warps_per_block", C.c_int)]
+
+
 # Every symbol include/depth_cuda.h declares: name -> (restype, argtypes).
 _vp, _i, _f, _sz = C.c_void_p, C.c_int, C.c_float, C.c_size_t
 SIGNATURES = {
@@ -63,6 +69,8 @@ SIGNATURES = {
     "ds_profile_enable": (_i, [_vp, _i]),
     "ds_profile_collect": (_i, [_vp, _vp, _i, C.POINTER(_i)]),
     "ds_kernel_launches": (C.c_uint64, []),
+    "ds_set_kernel_config": (_i, [_vp, C.POINTER(KernelConfigC)]),
+    "ds_get_kernel_config": (_i, [_vp, C.POINTER(KernelConfigC)]),
 }
 
 _lib = None

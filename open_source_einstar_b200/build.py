@@ -20,7 +20,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared", "-cudart", "static",
 ]
 
-SOURCES = ["depth_cuda.cu"]
+SOURCES = ["depth_cuda.cu", "inst_r1.cu", "inst_r2.cu", "inst_r3.cu", "inst_r4.cu", "inst_r6.cu", "inst_r8.cu"]
 
 
 def _nvcc() -> str:
@@ -43,7 +43,21 @@ def build_native(force: bool = False, verbose: bool = False) -> str:
     if not force and not _stale(LIB, deps):
         return LIB
     os.makedirs(LIB_DIR, exist_ok=True)
-    cmd = [_nvcc(), *NVCC_FLAGS, "-o", LIB, *[os.path.join(CSRC, s) for s in SOURCES]]
+    obj_dir = os.path.join(PKG, "_build")
+    os.makedirs(obj_dir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f not in ("-shared",)]
+    procs, objs = [], []
+    for src in SOURCES:
+        obj = os.path.join(obj_dir, src.replace(".cu", ".o"))
+        objs.append(obj)
+        cmd = [_nvcc(), *compile_flags, "-c", "-o", obj, os.path.join(CSRC, src)]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        procs.append((src, subprocess.Popen(cmd)))
+    failed = [src for src, p in procs if p.wait() != 0]
+    if failed:
+        raise RuntimeError(f"nvcc failed for {failed}")
+    cmd = [_nvcc(), *NVCC_FLAGS, "-o", LIB, *objs]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -10,7 +10,9 @@
 #include <vector>
 
 #include "../../include/depth_cuda.h"
-#include "stereo_kernels.cuh"
+#include "dispatch.h"
+#include "frame_kernels.cuh"
+#include "fused_kernels.cuh"
 
 namespace {
 
@@ -34,12 +36,21 @@ double now_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-int round_vpl(int nd) {
-    const int need = (nd + 31) / 32;
-    static const int kSteps[] = {1, 2, 3, 4, 6, 8, 12, 16};
-    for (int s : kSteps)
-        if (s >= need) return s;
-    return 16;
+// Default kernel configuration for D disparities: the fewest padded lanes, two scanlines per warp
+// (SEG 16) while D <= 96. ds_set_kernel_config overrides it (the autotuner does).
+ds::KernelCfg default_cfg(int nd) {
+    ds::KernelCfg c;
+    c.materialize = true;  // fastest measured on B200 for 1280x1024, D=128 (cost volume read by each direction)
+    c.prefetch = 8;
+    if (nd <= 32) c.R = 1, c.seg = 16;
+    else if (nd <= 64) c.R = 2, c.seg = 16;
+    else if (nd <= 96) c.R = 3, c.seg = 16;
+    else if (nd <= 128) c.R = 4, c.seg = 16;
+    else if (nd <= 192) c.R = 3, c.seg = 32;
+    else if (nd <= 256) c.R = 4, c.seg = 32;
+    else if (nd <= 384) c.R = 6, c.seg = 32;
+    else c.R = 8, c.seg = 32;
+    return c;
 }
 
 }  // namespace
@@ -47,9 +58,11 @@ int round_vpl(int nd) {
 struct ds_handle {
     ds_stereo_params p{};
     int w = 0, h = 0;
-    int nd = 0, vpl = 0, dp = 0, ndirs = 4;
+    int nd = 0, dp = 0, ndirs = 4;
+    ds::KernelCfg cfg{};
     bool wide = false;      // u16 path values
     bool census64 = false;  // u64 census words
+    bool s16 = false;       // fused pairs: u16 vertical sums (2 (window + P2) > 255 or wide)
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
@@ -61,6 +74,9 @@ struct ds_handle {
     void* d_census[2] = {nullptr, nullptr};
     void* d_values = nullptr;
     size_t dir_stride = 0;
+    size_t values_bytes = 0;
+    uint8_t* d_costs = nullptr;  // materialised costs (cfg.materialize)
+    size_t costs_bytes = 0;
     float* d_disp_lr = nullptr;
     float* d_out_disp = nullptr;
     float* d_out_conf = nullptr;
@@ -105,6 +121,7 @@ void release(ds_handle* h) {
     for (auto* p : h->d_map) f(p);
     for (auto* p : h->d_census) f(p);
     f(h->d_values);
+    f(h->d_costs);
     f(h->d_disp_lr);
     f(h->d_out_disp);
     f(h->d_out_conf);
@@ -151,35 +168,77 @@ int validate(const ds_stereo_params& p, int w, int h, std::string& msg) {
     return DS_OK;
 }
 
-template <int VPL, typename CW, typename ST>
-void launch_paths_t(const ds_handle* h, cudaStream_t st) {
+constexpr size_t kMaxSmem = 227 * 1024;
+
+size_t horz_smem(const ds_handle* h, const ds::KernelCfg& c) {
+    return static_cast<size_t>(c.horz_warps) * (32 / c.seg) * h->w * 8;
+}
+
+dsk::FusedArgs fused_args(const ds_handle* h) {
+    const auto& sg = h->p.sgm;
+    dsk::FusedArgs a{};
+    a.census_l = h->d_census[0];
+    a.census_r = h->d_census[1];
+    a.guide = h->d_rect[0];
+    a.S = h->d_values;
+    a.T = static_cast<uint8_t*>(h->d_values) + h->dir_stride * (h->s16 ? 2 : 1);
+    a.w = h->w;
+    a.h = h->h;
+    a.nd = h->nd;
+    a.dp = h->dp;
+    a.min_disp = sg.min_disparity;
+    a.p1 = sg.p1;
+    a.invalid_cost = (2 * sg.census_radius_x + 1) * (2 * sg.census_radius_y + 1);
+    a.slant = sg.slant_steps ? 1 : 0;
+    for (int q = 0; q < 32; ++q) a.p2_table[q] = sg.adaptive_p2 ? std::max(sg.p1 + 1, sg.p2 / (q + 1)) : sg.p2;
+    a.uniqueness = sg.uniqueness;
+    a.subpixel = h->p.subpixel ? 1 : 0;
+    a.lr_max_diff = sg.lr_max_diff;
+    a.disp = h->d_disp_lr;
+    return a;
+}
+
+void launch_paths(ds_handle* h, cudaStream_t st) {
+    if (h->cfg.fused) {
+        DS_CUDA(ds::launch_vert(h->cfg, h->census64, h->s16, fused_args(h), st));
+        ++g_launches;
+        return;
+    }
+    const auto& sg = h->p.sgm;
+    const int window = (2 * sg.census_radius_x + 1) * (2 * sg.census_radius_y + 1);
+    if (h->cfg.materialize) {
+        dsk::CostArgs c{h->d_census[0], h->d_census[1], h->d_costs, h->w, h->h, h->nd, h->dp, sg.min_disparity, window};
+        DS_CUDA(ds::launch_costs(h->cfg, h->census64, c, st));
+        ++g_launches;
+    }
     dsk::PathArgs a{};
     a.census_l = h->d_census[0];
     a.census_r = h->d_census[1];
     a.guide = h->d_rect[0];
+    a.costs = h->cfg.materialize ? h->d_costs : nullptr;
     a.values = h->d_values;
     a.dir_stride = h->dir_stride;
     a.w = h->w;
     a.h = h->h;
     a.nd = h->nd;
     a.dp = h->dp;
-    a.min_disp = h->p.sgm.min_disparity;
-    a.p1 = h->p.sgm.p1;
-    a.invalid_cost = (2 * h->p.sgm.census_radius_x + 1) * (2 * h->p.sgm.census_radius_y + 1);
-    a.slant = h->p.sgm.slant_steps ? 1 : 0;
+    a.min_disp = sg.min_disparity;
+    a.p1 = sg.p1;
+    a.invalid_cost = window;
+    a.slant = sg.slant_steps ? 1 : 0;
     a.dir_base = 0;
-    for (int q = 0; q < 32; ++q) {
-        const int adaptive = std::max(h->p.sgm.p1 + 1, h->p.sgm.p2 / (q + 1));
-        a.p2_table[q] = h->p.sgm.adaptive_p2 ? adaptive : h->p.sgm.p2;
-    }
-    const int wpb = 4;
+    for (int q = 0; q < 32; ++q) a.p2_table[q] = sg.adaptive_p2 ? std::max(sg.p1 + 1, sg.p2 / (q + 1)) : sg.p2;
     const int max_lines = h->ndirs == 8 ? h->w + h->h - 1 : std::max(h->w, h->h);
-    dim3 grid((max_lines + wpb - 1) / wpb, h->ndirs);
-    dsk::k_paths<VPL, CW, ST><<<grid, wpb * 32, 0, st>>>(a);
+    DS_CUDA(ds::launch_paths(h->cfg, h->census64, h->wide, a, h->ndirs, max_lines, st));
+    ++g_launches;
 }
 
-template <int VPL, typename ST>
-void launch_wta_t(const ds_handle* h, cudaStream_t st) {
+void launch_wta(ds_handle* h, cudaStream_t st) {
+    if (h->cfg.fused) {
+        DS_CUDA(ds::launch_horz(h->cfg, h->census64, h->s16, fused_args(h), horz_smem(h, h->cfg), st));
+        ++g_launches;
+        return;
+    }
     dsk::WtaArgs a{};
     a.values = h->d_values;
     a.dir_stride = h->dir_stride;
@@ -193,54 +252,38 @@ void launch_wta_t(const ds_handle* h, cudaStream_t st) {
     a.subpixel = h->p.subpixel ? 1 : 0;
     a.lr_max_diff = h->p.sgm.lr_max_diff;
     a.disp = h->d_disp_lr;
-    const size_t smem = static_cast<size_t>(h->w) * 8;
-    DS_CUDA(cudaFuncSetAttribute(dsk::k_wta<VPL, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-    dsk::k_wta<VPL, ST><<<h->h, 256, smem, st>>>(a);
-}
-
-template <int VPL>
-void paths_vpl(const ds_handle* h, cudaStream_t st) {
-    if (h->census64) {
-        if (h->wide) launch_paths_t<VPL, uint64_t, uint16_t>(h, st);
-        else launch_paths_t<VPL, uint64_t, uint8_t>(h, st);
-    } else {
-        if (h->wide) launch_paths_t<VPL, uint32_t, uint16_t>(h, st);
-        else launch_paths_t<VPL, uint32_t, uint8_t>(h, st);
-    }
+    DS_CUDA(ds::launch_wta(h->cfg, h->wide, a, h->h, static_cast<size_t>(h->w) * 8, st));
     ++g_launches;
 }
 
-template <int VPL>
-void wta_vpl(const ds_handle* h, cudaStream_t st) {
-    if (h->wide) launch_wta_t<VPL, uint16_t>(h, st);
-    else launch_wta_t<VPL, uint8_t>(h, st);
-    ++g_launches;
-}
-
-template <template <int> class Op>
-void by_vpl(const ds_handle* h, cudaStream_t st) {
-    switch (h->vpl) {
-        case 1: Op<1>::run(h, st); break;
-        case 2: Op<2>::run(h, st); break;
-        case 3: Op<3>::run(h, st); break;
-        case 4: Op<4>::run(h, st); break;
-        case 6: Op<6>::run(h, st); break;
-        case 8: Op<8>::run(h, st); break;
-        case 12: Op<12>::run(h, st); break;
-        default: Op<16>::run(h, st); break;
+// (Re)allocates the buffers whose size depends on the kernel configuration.
+void size_config_buffers(ds_handle* h) {
+    h->dp = h->cfg.dp();
+    const size_t n = static_cast<size_t>(h->w) * h->h;
+    h->dir_stride = n * static_cast<size_t>(h->dp);
+    const size_t vb = h->cfg.fused ? h->dir_stride * 2 * (h->s16 ? 2 : 1) : h->dir_stride * h->ndirs * (h->wide ? 2 : 1);
+    if (vb != h->values_bytes) {
+        if (h->d_values) {
+            cudaFree(h->d_values);
+            h->bytes -= h->values_bytes;
+            h->d_values = nullptr;
+            h->values_bytes = 0;
+        }
+        h->d_values = h->alloc<uint8_t>(vb);
+        h->values_bytes = vb;
+    }
+    const size_t cb = h->cfg.materialize && !h->cfg.fused ? n * static_cast<size_t>(h->dp) : 0;
+    if (cb != h->costs_bytes) {
+        if (h->d_costs) {
+            cudaFree(h->d_costs);
+            h->bytes -= h->costs_bytes;
+            h->d_costs = nullptr;
+            h->costs_bytes = 0;
+        }
+        if (cb) h->d_costs = h->alloc<uint8_t>(cb);
+        h->costs_bytes = cb;
     }
 }
-template <int V>
-struct PathsOp {
-    static void run(const ds_handle* h, cudaStream_t st) { paths_vpl<V>(h, st); }
-};
-template <int V>
-struct WtaOp {
-    static void run(const ds_handle* h, cudaStream_t st) { wta_vpl<V>(h, st); }
-};
-
-void launch_paths(const ds_handle* h, cudaStream_t st) { by_vpl<PathsOp>(h, st); }
-void launch_wta(const ds_handle* h, cudaStream_t st) { by_vpl<WtaOp>(h, st); }
 
 struct StageMarks {
     ds_handle* h;
@@ -391,6 +434,45 @@ int guarded(ds_handle* h, F&& f) {
 
 }  // namespace
 
+namespace ds {
+
+bool cfg_supported(int R, int seg) {
+    if (seg == 16) return R == 1 || R == 2 || R == 3 || R == 4;
+    if (seg == 32) return R == 1 || R == 2 || R == 3 || R == 4 || R == 6 || R == 8;
+    return false;
+}
+
+#define DS_BY_R(FN, ...)                        \
+    switch (cfg.R) {                            \
+        case 1: return FN##_r1(__VA_ARGS__);    \
+        case 2: return FN##_r2(__VA_ARGS__);    \
+        case 3: return FN##_r3(__VA_ARGS__);    \
+        case 4: return FN##_r4(__VA_ARGS__);    \
+        case 6: return FN##_r6(__VA_ARGS__);    \
+        case 8: return FN##_r8(__VA_ARGS__);    \
+        default: return cudaErrorInvalidValue;  \
+    }
+
+cudaError_t launch_paths(const KernelCfg& cfg, bool c64, bool wide, const dsk::PathArgs& a, int ndirs, int max_lines,
+                         cudaStream_t st) {
+    DS_BY_R(launch_paths, cfg, c64, wide, a, ndirs, max_lines, st)
+}
+cudaError_t launch_wta(const KernelCfg& cfg, bool wide, const dsk::WtaArgs& a, int rows, size_t smem, cudaStream_t st) {
+    DS_BY_R(launch_wta, cfg, wide, a, rows, smem, st)
+}
+cudaError_t launch_costs(const KernelCfg& cfg, bool c64, const dsk::CostArgs& a, cudaStream_t st) {
+    DS_BY_R(launch_costs, cfg, c64, a, st)
+}
+cudaError_t launch_vert(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, cudaStream_t st) {
+    DS_BY_R(launch_vert, cfg, c64, s16, a, st)
+}
+cudaError_t launch_horz(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, size_t smem, cudaStream_t st) {
+    DS_BY_R(launch_horz, cfg, c64, s16, a, smem, st)
+}
+#undef DS_BY_R
+
+}  // namespace ds
+
 extern "C" {
 
 DS_API void ds_default_params(ds_stereo_params* p) {
@@ -435,13 +517,18 @@ DS_API int ds_create(const ds_stereo_params* params, int width, int height, ds_h
         h->w = width;
         h->h = height;
         h->nd = params->sgm.num_disparities;
-        h->vpl = round_vpl(h->nd);
-        h->dp = 32 * h->vpl;
+        h->cfg = default_cfg(h->nd);
         h->ndirs = params->sgm.eight_paths ? 8 : 4;
         const int window = (2 * params->sgm.census_radius_x + 1) * (2 * params->sgm.census_radius_y + 1);
         h->census64 = window - 1 > 32;
         // Path values are at most window + P2 (the recurrence never lets best exceed min(prev) + P2).
         h->wide = params->wide_costs || window + params->sgm.p2 > 255;
+        h->s16 = h->wide || 2 * (window + params->sgm.p2) > 255;
+        h->cfg.fused = false;  // the fused pairs are selectable (ds_set_kernel_config / autotuner)
+        if (h->ndirs == 4) {
+            const int rows_max = static_cast<int>(kMaxSmem / (static_cast<size_t>(width) * 8));
+            h->cfg.horz_warps = std::max(1, std::min(4, rows_max / (32 / h->cfg.seg)));
+        }
         DS_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
         DS_CUDA(cudaEventCreate(&h->ev0));
         DS_CUDA(cudaEventCreate(&h->ev1));
@@ -451,8 +538,7 @@ DS_API int ds_create(const ds_stereo_params* params, int width, int height, ds_h
         const size_t cw = h->census64 ? 8 : 4;
         h->d_census[0] = h->alloc<uint8_t>(n * cw);
         h->d_census[1] = h->alloc<uint8_t>(n * cw);
-        h->dir_stride = n * static_cast<size_t>(h->dp);
-        h->d_values = h->alloc<uint8_t>(h->dir_stride * h->ndirs * (h->wide ? 2 : 1));
+        size_config_buffers(h);
         h->d_disp_lr = h->alloc<float>(n);
         h->d_out_disp = h->alloc<float>(n);
         h->d_out_conf = h->alloc<float>(n);
@@ -594,13 +680,46 @@ DS_API int ds_debug_read(ds_handle* h, uint64_t* census_left, uint64_t* census_r
             const size_t m = n * h->nd;
             uint16_t* d = nullptr;
             DS_CUDA(cudaMalloc(&d, m * 2));
-            dsk::SumArgs a{h->d_values, h->dir_stride, h->ndirs, h->w, h->h, h->nd, h->dp, d};
-            if (h->wide) dsk::k_debug_sums<uint16_t><<<1024, 256, 0, h->stream>>>(a);
-            else dsk::k_debug_sums<uint8_t><<<1024, 256, 0, h->stream>>>(a);
-            cudaError_t e = cudaGetLastError();
+            void* vals = h->d_values;
+            void* tmp = nullptr;
+            cudaError_t e = cudaSuccess;
+            if (h->cfg.fused) {
+                // The fused pairs keep no per-direction values: recompute them with the per-direction kernel.
+                e = cudaMalloc(&tmp, h->dir_stride * h->ndirs * (h->wide ? 2 : 1));
+                if (e == cudaSuccess) {
+                    ds::KernelCfg gc = h->cfg;
+                    gc.fused = false;
+                    gc.materialize = false;
+                    const auto& sg = h->p.sgm;
+                    dsk::PathArgs pa{};
+                    pa.census_l = h->d_census[0];
+                    pa.census_r = h->d_census[1];
+                    pa.guide = h->d_rect[0];
+                    pa.values = tmp;
+                    pa.dir_stride = h->dir_stride;
+                    pa.w = h->w;
+                    pa.h = h->h;
+                    pa.nd = h->nd;
+                    pa.dp = h->dp;
+                    pa.min_disp = sg.min_disparity;
+                    pa.p1 = sg.p1;
+                    pa.invalid_cost = (2 * sg.census_radius_x + 1) * (2 * sg.census_radius_y + 1);
+                    pa.slant = sg.slant_steps ? 1 : 0;
+                    for (int q = 0; q < 32; ++q) pa.p2_table[q] = sg.adaptive_p2 ? std::max(sg.p1 + 1, sg.p2 / (q + 1)) : sg.p2;
+                    e = ds::launch_paths(gc, h->census64, h->wide, pa, h->ndirs, std::max(h->w, h->h), h->stream);
+                    vals = tmp;
+                }
+            }
+            dsk::SumArgs a{vals, h->dir_stride, h->ndirs, h->w, h->h, h->nd, h->dp, d};
+            if (e == cudaSuccess) {
+                if (h->wide) dsk::k_debug_sums<uint16_t><<<1024, 256, 0, h->stream>>>(a);
+                else dsk::k_debug_sums<uint8_t><<<1024, 256, 0, h->stream>>>(a);
+                e = cudaGetLastError();
+            }
             if (e == cudaSuccess) e = cudaMemcpyAsync(path_sums, d, m * 2, cudaMemcpyDeviceToHost, h->stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
             cudaFree(d);
+            if (tmp) cudaFree(tmp);
             if (e != cudaSuccess) throw CudaFailure{e, "debug sums"};
         }
         return DS_OK;
@@ -645,5 +764,52 @@ DS_API int ds_profile_collect(ds_handle* h, double* stage_ms, int max_frames, in
 }
 
 DS_API uint64_t ds_kernel_launches(void) { return g_launches.load(); }
+
+DS_API int ds_set_kernel_config(ds_handle* h, const ds_kernel_config* c) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    if (!c) return h->fail(DS_INVALID_ARGUMENT, "null kernel config");
+    if (!ds::cfg_supported(c->regs_per_lane, c->lanes_per_line))
+        return h->fail(DS_INVALID_ARGUMENT, "unsupported kernel configuration (lanes per line 16: R 1-4; 32: R 1,2,3,4,6,8)");
+    if (c->lanes_per_line * 2 * c->regs_per_lane < h->nd)
+        return h->fail(DS_INVALID_ARGUMENT, "kernel configuration holds fewer disparities than num_disparities");
+    if (c->path_warps_per_block < 1 || c->path_warps_per_block > 8 || c->wta_threads < 32 || c->wta_threads > 256 ||
+        c->wta_threads % 32 || (c->prefetch_steps != 4 && c->prefetch_steps != 8))
+        return h->fail(DS_INVALID_ARGUMENT, "block shape or prefetch depth out of range");
+    if (c->fused_pairs) {
+        if (h->ndirs != 4) return h->fail(DS_INVALID_ARGUMENT, "fused pairs need 4 paths");
+        if (c->path_warps_per_block > 4 || c->horz_warps_per_block < 1 || c->horz_warps_per_block > 4)
+            return h->fail(DS_INVALID_ARGUMENT, "fused pairs: 1..4 warps per direction per block");
+        ds::KernelCfg t;
+        t.seg = c->lanes_per_line;
+        t.horz_warps = c->horz_warps_per_block;
+        if (horz_smem(h, t) > kMaxSmem) return h->fail(DS_INVALID_ARGUMENT, "fused pairs: rows per block exceed shared memory");
+    }
+    return guarded(h, [&]() -> int {
+        DS_CUDA(cudaStreamSynchronize(h->stream));
+        h->cfg.R = c->regs_per_lane;
+        h->cfg.seg = c->lanes_per_line;
+        h->cfg.materialize = c->materialize_costs != 0;
+        h->cfg.paths_warps = c->path_warps_per_block;
+        h->cfg.wta_threads = c->wta_threads;
+        h->cfg.prefetch = c->prefetch_steps;
+        h->cfg.fused = c->fused_pairs != 0;
+        h->cfg.horz_warps = c->horz_warps_per_block;
+        size_config_buffers(h);
+        return DS_OK;
+    });
+}
+
+DS_API int ds_get_kernel_config(const ds_handle* h, ds_kernel_config* c) {
+    if (!h || !c) return DS_INVALID_ARGUMENT;
+    c->regs_per_lane = h->cfg.R;
+    c->lanes_per_line = h->cfg.seg;
+    c->materialize_costs = h->cfg.materialize ? 1 : 0;
+    c->path_warps_per_block = h->cfg.paths_warps;
+    c->wta_threads = h->cfg.wta_threads;
+    c->prefetch_steps = h->cfg.prefetch;
+    c->fused_pairs = h->cfg.fused ? 1 : 0;
+    c->horz_warps_per_block = h->cfg.horz_warps;
+    return DS_OK;
+}
 
 }  // extern "C"

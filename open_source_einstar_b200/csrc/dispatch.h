@@ -1,0 +1,60 @@
+// Host-side launch of the SGM kernels for one kernel configuration. The kernels are templates over the
+// per-lane register count R (2R disparities per lane), the segment width SEG (lanes per scanline / per
+// pixel), the census word, the path-value storage type and cost materialisation; each R is
+// instantiated in its own translation unit (inst_r*.cu) so that the library builds in parallel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace dsk {
+struct PathArgs;
+struct WtaArgs;
+struct CostArgs;
+struct FusedArgs;
+}  // namespace dsk
+
+namespace ds {
+
+// A kernel configuration: 2R disparities per lane, SEG lanes per scanline (16: two lines per warp).
+struct KernelCfg {
+    int R = 2;
+    int seg = 32;
+    bool materialize = false;  // cost volume written once and read by every direction
+    int paths_warps = 4;       // warps per block of the path kernel
+    int prefetch = 4;          // steps of inputs in flight per scanline (4 or 8)
+    int wta_threads = 256;     // threads per block of the WTA kernel
+    bool fused = true;         // 4 paths as two meet-in-the-middle pairs with the WTA fused (k_vert, k_horz_wta)
+    int horz_warps = 4;        // fused: warps per direction per block of k_horz_wta (rows = horz_warps * 32/SEG)
+    int dp() const { return seg * 2 * R; }
+};
+
+// Configurations that have kernels: SEG 16 with R in {1,2,3,4}; SEG 32 with R in {1,2,3,4,6,8}.
+bool cfg_supported(int R, int seg);
+
+// Returns a CUDA error (cudaSuccess on success). `c64`: 64-bit census words; `wide`: u16 path values.
+cudaError_t launch_paths(const KernelCfg& cfg, bool c64, bool wide, const dsk::PathArgs& a, int ndirs, int max_lines,
+                         cudaStream_t st);
+cudaError_t launch_wta(const KernelCfg& cfg, bool wide, const dsk::WtaArgs& a, int rows, size_t smem, cudaStream_t st);
+cudaError_t launch_costs(const KernelCfg& cfg, bool c64, const dsk::CostArgs& a, cudaStream_t st);
+// Fused pairs: `s16` = 16-bit vertical sums / horizontal scratch.
+cudaError_t launch_vert(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, cudaStream_t st);
+cudaError_t launch_horz(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, size_t smem, cudaStream_t st);
+
+#define DS_DECLARE_R(R)                                                                                              \
+    cudaError_t launch_paths_r##R(const KernelCfg&, bool, bool, const dsk::PathArgs&, int, int, cudaStream_t);      \
+    cudaError_t launch_wta_r##R(const KernelCfg&, bool, const dsk::WtaArgs&, int, size_t, cudaStream_t);              \
+    cudaError_t launch_costs_r##R(const KernelCfg&, bool, const dsk::CostArgs&, cudaStream_t);                      \
+    cudaError_t launch_vert_r##R(const KernelCfg&, bool, bool, const dsk::FusedArgs&, cudaStream_t);                \
+    cudaError_t launch_horz_r##R(const KernelCfg&, bool, bool, const dsk::FusedArgs&, size_t, cudaStream_t);
+DS_DECLARE_R(1)
+DS_DECLARE_R(2)
+DS_DECLARE_R(3)
+DS_DECLARE_R(4)
+DS_DECLARE_R(6)
+DS_DECLARE_R(8)
+#undef DS_DECLARE_R
+
+}  // namespace ds

@@ -1,0 +1,181 @@
+// Per-frame kernels around the SGM core (sm_100a): rectification remap, census, median + outputs.
+// Included by one translation unit only (depth_cuda.cu).
+#pragma once
+
+#include "stereo_kernels.cuh"
+
+namespace dsk {
+
+// ------------------------------------------------------------------------------------------------
+// Rectification: bilinear remap (libs/calib/src/rectify.cpp:133-148), optionally followed by the
+// 2x2 box downsample of depth::downsample2 (stereo.cpp:348-359) when the tables are twice the size.
+
+struct RectifyArgs {
+    const uint8_t* raw[2];
+    const float* map_x[2];
+    const float* map_y[2];
+    uint8_t* out[2];
+    int raw_w, raw_h;
+    int map_w;
+    int out_w, out_h;
+    int half;
+};
+
+__device__ __forceinline__ uint32_t remap_sample(const uint8_t* __restrict__ src, int sw, int sh, float sx, float sy) {
+    const int x0 = static_cast<int>(floorf(sx)), y0 = static_cast<int>(floorf(sy));
+    if (x0 < 0 || y0 < 0 || x0 + 1 >= sw || y0 + 1 >= sh) return 0u;
+    const float fx = __fsub_rn(sx, static_cast<float>(x0));
+    const float fy = __fsub_rn(sy, static_cast<float>(y0));
+    const float gx = __fsub_rn(1.0f, fx), gy = __fsub_rn(1.0f, fy);
+    const uint8_t* r0 = src + static_cast<size_t>(y0) * sw + x0;
+    const uint8_t* r1 = r0 + sw;
+    const float a = __ldg(r0), b = __ldg(r0 + 1), c = __ldg(r1), d = __ldg(r1 + 1);
+    const float top = __fadd_rn(__fmul_rn(a, gx), __fmul_rn(b, fx));
+    const float bot = __fadd_rn(__fmul_rn(c, gx), __fmul_rn(d, fx));
+    float v = __fadd_rn(__fmul_rn(top, gy), __fmul_rn(bot, fy));
+    v = fminf(fmaxf(__fadd_rn(v, 0.5f), 0.0f), 255.0f);
+    return static_cast<uint32_t>(__float2uint_rz(v));
+}
+
+__global__ void k_rectify(RectifyArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int side = blockIdx.z;
+    if (x >= a.out_w || y >= a.out_h) return;
+    const uint8_t* src = a.raw[side];
+    const float* mx = a.map_x[side];
+    const float* my = a.map_y[side];
+    uint32_t v;
+    if (!a.half) {
+        const size_t i = static_cast<size_t>(y) * a.map_w + x;
+        v = remap_sample(src, a.raw_w, a.raw_h, __ldg(mx + i), __ldg(my + i));
+    } else {
+        uint32_t acc = 0;
+        for (int j = 0; j < 2; ++j)
+            for (int i = 0; i < 2; ++i) {
+                const size_t m = static_cast<size_t>(2 * y + j) * a.map_w + (2 * x + i);
+                acc += remap_sample(src, a.raw_w, a.raw_h, __ldg(mx + m), __ldg(my + m));
+            }
+        v = (acc + 2u) / 4u;
+    }
+    a.out[side][static_cast<size_t>(y) * a.out_w + x] = static_cast<uint8_t>(v);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Census (stereo.cpp:328-346): bit per window neighbour, row-major, centre skipped, MSB first,
+// set when neighbour < centre; 0 within (rx, ry) of the border.
+
+struct CensusArgs {
+    const uint8_t* img[2];
+    void* out[2];
+    int w, h, rx, ry;
+};
+
+template <typename W>
+__global__ void k_census(CensusArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int side = blockIdx.z;
+    if (x >= a.w || y >= a.h) return;
+    const uint8_t* img = a.img[side];
+    W word = 0;
+    if (y >= a.ry && y < a.h - a.ry && x >= a.rx && x < a.w - a.rx) {
+        const uint8_t c = __ldg(img + static_cast<size_t>(y) * a.w + x);
+        for (int v = -a.ry; v <= a.ry; ++v) {
+            const uint8_t* row = img + static_cast<size_t>(y + v) * a.w + x;
+            for (int u = -a.rx; u <= a.rx; ++u) {
+                if (u == 0 && v == 0) continue;
+                word = static_cast<W>((word << 1) | static_cast<W>(__ldg(row + u) < c));
+            }
+        }
+    }
+    static_cast<W*>(a.out[side])[static_cast<size_t>(y) * a.w + x] = word;
+}
+
+// ------------------------------------------------------------------------------------------------
+// 3x3 median (stereo.cpp:129-147) + outputs: f32 disparity, confidence (stereo.cpp:515-519), u16
+// disparity, depth z = f B / (d + cx_offset) in double with the gates of point_image.cpp:18-20.
+
+struct PostArgs {
+    const float* disp;
+    int w, h, median, min_disp;
+    float* out_disp;
+    float* out_conf;
+    uint16_t* out_u16;
+    float* out_depth;
+    double f, baseline, cx_offset;
+    float min_depth, max_depth;
+};
+
+__global__ void k_post(PostArgs a) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= a.w || y >= a.h) return;
+    const size_t i = static_cast<size_t>(y) * a.w + x;
+    float d = __ldg(a.disp + i);
+    if (a.median && valid_disparity(d)) {
+        float v[9];
+        int n = 0;
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int xx = x + dx, yy = y + dy;
+                if (xx < 0 || yy < 0 || xx >= a.w || yy >= a.h) continue;
+                const float q = __ldg(a.disp + static_cast<size_t>(yy) * a.w + xx);
+                if (!valid_disparity(q)) continue;
+                int p = n++;
+                while (p > 0 && v[p - 1] > q) {
+                    v[p] = v[p - 1];
+                    --p;
+                }
+                v[p] = q;
+            }
+        d = v[n / 2];
+    }
+    const bool ok = valid_disparity(d);
+    if (a.out_disp) a.out_disp[i] = d;
+    if (a.out_conf) a.out_conf[i] = ok ? 1.0f : 0.0f;
+    if (a.out_u16) {
+        uint16_t u = 0xFFFFu;
+        if (ok) {
+            const float q = __fmul_rn(__fsub_rn(d, static_cast<float>(a.min_disp)), 64.0f);
+            const int r = min(max(__float2int_rn(q), 0), 0xFFFE);
+            u = static_cast<uint16_t>(r);
+        }
+        a.out_u16[i] = u;
+    }
+    if (a.out_depth) {
+        float z = 0.0f;
+        if (ok) {
+            const double dd = __dadd_rn(static_cast<double>(d), a.cx_offset);
+            if (dd > 0.0) {
+                const double zz = __ddiv_rn(__dmul_rn(a.f, a.baseline), dd);
+                if (!(zz < static_cast<double>(a.min_depth) || zz > static_cast<double>(a.max_depth)))
+                    z = __double2float_rn(zz);
+            }
+        }
+        a.out_depth[i] = z;
+    }
+}
+
+// Debug: summed path values as u16 [y][x][nd] (the reference's `sum` volume).
+struct SumArgs {
+    const void* values;
+    size_t dir_stride;
+    int ndirs, w, h, nd, dp;
+    uint16_t* out;
+};
+
+template <typename ST>
+__global__ void k_debug_sums(SumArgs a) {
+    const size_t n = static_cast<size_t>(a.w) * a.h * a.nd;
+    const ST* v = static_cast<const ST*>(a.values);
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const size_t px = i / a.nd;
+        const int k = static_cast<int>(i % a.nd);
+        uint32_t s = 0;
+        for (int d = 0; d < a.ndirs; ++d) s += v[static_cast<size_t>(d) * a.dir_stride + px * a.dp + k];
+        a.out[i] = static_cast<uint16_t>(s);
+    }
+}
+
+}  // namespace dsk

@@ -1,0 +1,127 @@
+// Template launchers behind dispatch.h, instantiated per R by inst_r*.cu.
+#pragma once
+
+#include "dispatch.h"
+#include "fused_kernels.cuh"
+#include "stereo_kernels.cuh"
+
+namespace ds {
+
+template <int R, int SEG, typename CW, typename ST, bool MAT>
+cudaError_t paths_t(const KernelCfg& cfg, const dsk::PathArgs& a, int ndirs, int max_lines, cudaStream_t st) {
+    const int lines_per_block = cfg.paths_warps * (32 / SEG);
+    dim3 grid((max_lines + lines_per_block - 1) / lines_per_block, ndirs);
+    if (cfg.prefetch == 8) dsk::k_paths<R, SEG, CW, ST, MAT, 8><<<grid, cfg.paths_warps * 32, 0, st>>>(a);
+    else dsk::k_paths<R, SEG, CW, ST, MAT, 4><<<grid, cfg.paths_warps * 32, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int R, int SEG>
+cudaError_t paths_seg(const KernelCfg& cfg, bool c64, bool wide, const dsk::PathArgs& a, int ndirs, int max_lines,
+                      cudaStream_t st) {
+    if (cfg.materialize) {
+        return wide ? paths_t<R, SEG, uint32_t, uint16_t, true>(cfg, a, ndirs, max_lines, st)
+                    : paths_t<R, SEG, uint32_t, uint8_t, true>(cfg, a, ndirs, max_lines, st);
+    }
+    if (c64) {
+        return wide ? paths_t<R, SEG, uint64_t, uint16_t, false>(cfg, a, ndirs, max_lines, st)
+                    : paths_t<R, SEG, uint64_t, uint8_t, false>(cfg, a, ndirs, max_lines, st);
+    }
+    return wide ? paths_t<R, SEG, uint32_t, uint16_t, false>(cfg, a, ndirs, max_lines, st)
+                : paths_t<R, SEG, uint32_t, uint8_t, false>(cfg, a, ndirs, max_lines, st);
+}
+
+template <int R, int SEG, typename ST>
+cudaError_t wta_t(const KernelCfg& cfg, const dsk::WtaArgs& a, int rows, size_t smem, cudaStream_t st) {
+    auto k = a.ndirs == 8 ? dsk::k_wta<R, SEG, ST, 8> : dsk::k_wta<R, SEG, ST, 4>;
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+    }
+    k<<<rows, cfg.wta_threads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int R, int SEG, typename CW>
+cudaError_t costs_t(const dsk::CostArgs& a, cudaStream_t st) {
+    const long px = static_cast<long>(a.w) * a.h;
+    const long px_per_block = 8 * (32 / SEG);
+    dsk::k_costs<R, SEG, CW><<<static_cast<unsigned>((px + px_per_block - 1) / px_per_block), 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int R, int SEG, typename CW, typename SV>
+cudaError_t vert_t(const KernelCfg& cfg, const dsk::FusedArgs& a, cudaStream_t st) {
+    const int nwd = cfg.paths_warps;
+    const int cols = nwd * (32 / SEG);
+    const dim3 grid((a.w + cols - 1) / cols);
+    if (cfg.prefetch == 8) dsk::k_vert<R, SEG, CW, SV, 8><<<grid, 64 * nwd, 0, st>>>(a);
+    else dsk::k_vert<R, SEG, CW, SV, 4><<<grid, 64 * nwd, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int R, int SEG, typename CW, typename SV>
+cudaError_t horz_t(const KernelCfg& cfg, const dsk::FusedArgs& a, size_t smem, cudaStream_t st) {
+    const int nrw = cfg.horz_warps;
+    const int rows = nrw * (32 / SEG);
+    const dim3 grid((a.h + rows - 1) / rows);
+    auto k = cfg.prefetch == 8 ? dsk::k_horz_wta<R, SEG, CW, SV, 8> : dsk::k_horz_wta<R, SEG, CW, SV, 4>;
+    if (smem > 48 * 1024) {
+        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        if (e != cudaSuccess) return e;
+    }
+    k<<<grid, 64 * nrw, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int R, int SEG>
+cudaError_t vert_seg(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, cudaStream_t st) {
+    if (c64) return s16 ? vert_t<R, SEG, uint64_t, uint16_t>(cfg, a, st) : vert_t<R, SEG, uint64_t, uint8_t>(cfg, a, st);
+    return s16 ? vert_t<R, SEG, uint32_t, uint16_t>(cfg, a, st) : vert_t<R, SEG, uint32_t, uint8_t>(cfg, a, st);
+}
+
+template <int R, int SEG>
+cudaError_t horz_seg(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, size_t smem, cudaStream_t st) {
+    if (c64)
+        return s16 ? horz_t<R, SEG, uint64_t, uint16_t>(cfg, a, smem, st) : horz_t<R, SEG, uint64_t, uint8_t>(cfg, a, smem, st);
+    return s16 ? horz_t<R, SEG, uint32_t, uint16_t>(cfg, a, smem, st) : horz_t<R, SEG, uint32_t, uint8_t>(cfg, a, smem, st);
+}
+
+}  // namespace ds
+
+// SEG 16 exists for R <= 4 only.
+#define DS_SEG_SWITCH(R, CALL16, CALL32) \
+    if (cfg.seg == 16) {                 \
+        if constexpr (R <= 4) return CALL16; \
+        return cudaErrorInvalidValue;    \
+    }                                    \
+    return CALL32;
+
+#define DS_DEFINE_R(R)                                                                                               \
+    namespace ds {                                                                                                   \
+    cudaError_t launch_paths_r##R(const KernelCfg& cfg, bool c64, bool wide, const dsk::PathArgs& a, int ndirs,      \
+                                  int max_lines, cudaStream_t st) {                                                  \
+        DS_SEG_SWITCH(R, (paths_seg<R, (R <= 4 ? 16 : 32)>(cfg, c64, wide, a, ndirs, max_lines, st)),               \
+                      (paths_seg<R, 32>(cfg, c64, wide, a, ndirs, max_lines, st)))                                   \
+    }                                                                                                                \
+    cudaError_t launch_wta_r##R(const KernelCfg& cfg, bool wide, const dsk::WtaArgs& a, int rows, size_t smem,       \
+                                cudaStream_t st) {                                                                   \
+        DS_SEG_SWITCH(R,                                                                                             \
+                      (wide ? wta_t<R, (R <= 4 ? 16 : 32), uint16_t>(cfg, a, rows, smem, st)                         \
+                            : wta_t<R, (R <= 4 ? 16 : 32), uint8_t>(cfg, a, rows, smem, st)),                        \
+                      (wide ? wta_t<R, 32, uint16_t>(cfg, a, rows, smem, st) : wta_t<R, 32, uint8_t>(cfg, a, rows, smem, st))) \
+    }                                                                                                                \
+    cudaError_t launch_costs_r##R(const KernelCfg& cfg, bool c64, const dsk::CostArgs& a, cudaStream_t st) {         \
+        DS_SEG_SWITCH(R,                                                                                             \
+                      (c64 ? costs_t<R, (R <= 4 ? 16 : 32), uint64_t>(a, st) : costs_t<R, (R <= 4 ? 16 : 32), uint32_t>(a, st)), \
+                      (c64 ? costs_t<R, 32, uint64_t>(a, st) : costs_t<R, 32, uint32_t>(a, st)))                     \
+    }                                                                                                                \
+    cudaError_t launch_vert_r##R(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, cudaStream_t st) { \
+        DS_SEG_SWITCH(R, (vert_seg<R, (R <= 4 ? 16 : 32)>(cfg, c64, s16, a, st)), (vert_seg<R, 32>(cfg, c64, s16, a, st))) \
+    }                                                                                                                \
+    cudaError_t launch_horz_r##R(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, size_t smem,     \
+                                 cudaStream_t st) {                                                                  \
+        DS_SEG_SWITCH(R, (horz_seg<R, (R <= 4 ? 16 : 32)>(cfg, c64, s16, a, smem, st)),                              \
+                      (horz_seg<R, 32>(cfg, c64, s16, a, smem, st)))                                                 \
+    }                                                                                                                \
+    }

@@ -266,6 +266,8 @@ class CudaStereo:
         o = N.OutputsC(*[_ptr(outputs.get(k)) for k in ("disparity", "confidence", "disparity_u16", "depth",
                                                         "rect_left", "rect_right")])
         s = None if stream is None else (stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+        if stream is not None and not s:
+            s = CUDA_STREAM_LEGACY  # torch's default stream is the legacy stream; NULL would mean the handle's
         fn = N.lib().ds_compute_raw_device if raw else N.lib().ds_compute_device
         self._check(fn(self._h, _ptr(left), _ptr(right), C.byref(o), s))
 
@@ -288,6 +290,19 @@ class CudaStereo:
     def device_bytes(self) -> int:
         return int(N.lib().ds_device_bytes(self._h))
 
+    def set_kernel_config(self, regs_per_lane: int, lanes_per_line: int, materialize_costs: bool = False,
+                          path_warps_per_block: int = 4, wta_threads: int = 256, prefetch_steps: int = 4,
+                          fused_pairs: bool = False, horz_warps_per_block: int = 4) -> None:
+        """ds_set_kernel_config: lanes per scanline (16/32) x 2*regs disparities per lane; results do not change."""
+        c = N.KernelConfigC(regs_per_lane, lanes_per_line, int(bool(materialize_costs)), path_warps_per_block, wta_threads,
+                            prefetch_steps, int(bool(fused_pairs)), horz_warps_per_block)
+        self._check(N.lib().ds_set_kernel_config(self._h, C.byref(c)))
+
+    def kernel_config(self) -> dict:
+        c = N.KernelConfigC()
+        self._check(N.lib().ds_get_kernel_config(self._h, C.byref(c)))
+        return {k: getattr(c, k) for k, _ in c._fields_}
+
     def profile(self, on: bool = True) -> None:
         """Per-stage CUDA events for every frame (stages: rectify, census, paths, wta+lr, median+outputs)."""
         self._check(N.lib().ds_profile_enable(self._h, int(bool(on))))
@@ -300,6 +315,7 @@ class CudaStereo:
         return buf[:n.value].copy()
 
 
+CUDA_STREAM_LEGACY = 1  # (cudaStream_t)0x1
 STAGES = 5
 STAGE_NAMES = ("rectify", "census", "paths", "wta_lr", "median_out")
 

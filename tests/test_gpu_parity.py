@@ -190,3 +190,46 @@ def test_errors_follow_the_reference(cuda, golden):
         # the handle stays usable after rejected calls
         r = s.compute(c["left"], c["right"])
         assert same_bits(r.disparity, c["disparity"])
+
+
+SUPPORTED = [(r, 16) for r in (1, 2, 3, 4)] + [(r, 32) for r in (1, 2, 3, 4, 6, 8)]
+
+
+@pytest.mark.parametrize("mode", ["per_direction", "materialized", "fused_pairs"])
+def test_every_kernel_config_is_bit_exact(cuda, golden, port, mode):
+    """All (lanes per line, regs per lane) configurations and all SGM kernel modes give identical bytes."""
+    for name in ("plane_sphere_160x128", "d_not_multiple_of_32_d40", "eight_paths", "census_9x7_wide", "tiny_37x29_d5",
+                 "census_7x7_u64", "negative_min_disparity", "no_subpixel_uniq08_lr2"):
+        c = golden[name]
+        p = OracleSgm(**c["params"])
+        if mode == "fused_pairs" and p.eight_paths:
+            continue
+        h, w = c["shape"]
+        want = c["median"]
+        for r, seg in SUPPORTED:
+            if 2 * r * seg < p.num_disparities:
+                continue
+            for pf in (4, 8):
+                with _stereo(p, w, h, c["subpixel"], median=True) as s:
+                    s.set_kernel_config(r, seg, mode == "materialized", path_warps_per_block=2 if r > 4 else 4,
+                                        wta_threads=128, prefetch_steps=pf, fused_pairs=mode == "fused_pairs",
+                                        horz_warps_per_block=2)
+                    got = s.compute(c["left"], c["right"]).disparity
+                assert same_bits(got, want), f"{name} R={r} SEG={seg} {mode} PF={pf}: {mismatch_report(got, want)}"
+
+
+@pytest.mark.parametrize("w,h,nd,mind", [(75, 41, 24, 3), (33, 7, 40, 0), (129, 2, 16, 5), (1, 9, 4, 0), (9, 1, 4, 0)])
+def test_odd_and_degenerate_sizes(cuda, port, w, h, nd, mind):
+    """Odd sizes split the meet-in-the-middle sweeps unevenly; 1-pixel rows/columns have one-step lines."""
+    rng = np.random.default_rng(w * 1000 + h)
+    base = (rng.random((h, w + 40)) * 255).astype(np.uint8)
+    left = base[:, 20:20 + w].copy()
+    right = base[:, 14:14 + w].copy()
+    p = OracleSgm(min_disparity=mind, num_disparities=nd)
+    want = port.median3(port.sgm_disparity(left, right, p))
+    for fused in (False, True):
+        with _stereo(p, w, h, median=True) as s:
+            cfg = s.kernel_config()
+            s.set_kernel_config(cfg["regs_per_lane"], cfg["lanes_per_line"], False, 1, 64, 4, fused, 1)
+            got = s.compute(left, right).disparity
+        assert same_bits(got, want), f"{w}x{h} fused={fused}: {mismatch_report(got, want)}"
