@@ -195,7 +195,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--frames", type=int, default=8, help="frames per step")
+    ap.add_argument("--frames", type=int, default=16, help="frames per step (the batch)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-budget", type=float, default=150.0, help="seconds of timed reference work at most")
     ap.add_argument("--kernel-config", default="", help="R,SEG,MATERIALIZE override (default: the library's choice)")
@@ -205,7 +205,9 @@ def main():
         return run_reference(args, world, rank)
 
     import torch
-    from open_source_einstar_b200 import CudaStereo, RectifiedGeometry, RemapTable, SgmParams, StereoParams, StereoResult
+    from open_source_einstar_b200 import (CudaStereo, PairDesc, RectifiedGeometry, RemapTable, SgmParams, StereoBatch,
+                                          StereoParams)
+    from open_source_einstar_b200.batch import BATCH_STAGE_NAMES
     from open_source_einstar_b200.stereo import STAGE_NAMES, kernel_launches
 
     torch.cuda.set_device(local)
@@ -219,100 +221,132 @@ def main():
     pairs = make_frames(B, 100 * rank, dev)
     (lx, ly), (rx, ry) = pairs[0].maps
     sp = StereoParams(sgm=SgmParams(min_disparity=pairs[0].min_disparity, num_disparities=D))
-    s = CudaStereo.create(sp, W, H)
-    s.set_rectification(RemapTable(lx, ly), RemapTable(rx, ry), W, H)
-    s.set_point_params(RectifiedGeometry(pairs[0].f, 0, 0, pairs[0].baseline, 0.0), 150.0, 700.0)
-
+    geom = RectifiedGeometry(pairs[0].f, 0, 0, pairs[0].baseline, 0.0)
+    kcfg = None
     if args.kernel_config:
         r, seg, mat = (int(v) for v in args.kernel_config.split(","))
-        s.set_kernel_config(r, seg, bool(mat))
+        kcfg = {"regs_per_lane": r, "lanes_per_line": seg, "materialize_costs": mat, "prefetch_steps": 8}
     raw = [(torch.from_numpy(p.left).to(dev), torch.from_numpy(p.right).to(dev)) for p in pairs]
     outs = [{"disparity_u16": torch.empty((H, W), dtype=torch.int16, device=dev),
              "depth": torch.empty((H, W), dtype=torch.float32, device=dev)} for _ in range(B)]
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
 
-    def step():
-        for (l, r), o in zip(raw, outs):
-            s.compute_device(l, r, o, stream=stream, raw=True)
-
     def barrier():
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize(dev)
 
-    clk = ClockSampler(local).__enter__()
-    for _ in range(args.warmup):
-        step()
-    barrier()
+    def max_over_ranks(v: float) -> float:
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
 
-    # ---- device-timed region -------------------------------------------------------------------------
+    clk = ClockSampler(local).__enter__()
+
+    # ---- per-frame launch path: one handle, frames back to back on one stream ----------------------------
+    s = CudaStereo.create(sp, W, H)
+    s.set_rectification(RemapTable(lx, ly), RemapTable(rx, ry), W, H)
+    s.set_point_params(geom, 150.0, 700.0)
+    if kcfg:
+        s.set_kernel_config(kcfg["regs_per_lane"], kcfg["lanes_per_line"], bool(kcfg["materialize_costs"]), 4, 256, 8)
+
+    def frame_step():
+        for (l, r), o in zip(raw, outs):
+            s.compute_device(l, r, o, stream=stream, raw=True)
+
+    for _ in range(args.warmup):
+        frame_step()
+    barrier()
     s.profile(True)
     s.profile_collect()
-    launches0 = kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     e0.record(stream)
     for _ in range(args.steps):
-        step()
+        frame_step()
     e1.record(stream)
     barrier()
-    launches = kernel_launches() - launches0
-    ms = e0.elapsed_time(e1)
+    pf_ms = max_over_ranks(e0.elapsed_time(e1))
     stages = s.profile_collect(max_frames=B * args.steps + 8)
     s.profile(False)
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
-    frames_total = B * args.steps * world
-    value = frames_total * PX_D / (ms_max * 1e-3) / 1e9
+    frame_tot = stages.sum(axis=1) if len(stages) else np.zeros(1)
+    per_frame_value = B * args.steps * world * PX_D / (pf_ms * 1e-3) / 1e9
 
-    # ---- end to end through the public host API (pinned host buffers) -------------------------------------
+    # ---- batched path: all frames in one graph replay (persistent launches) -----------------------------
+    desc = [PairDesc(W, H, sp, raw=True, calib=0, geometry=geom, kernel=kcfg) for _ in range(B)]
+    batch = StereoBatch(desc, n_calib=1)
+    batch.set_rectification(0, RemapTable(lx, ly), RemapTable(rx, ry), W, H)
+    bouts = [{"disparity_u16": torch.empty((H, W), dtype=torch.int16, device=dev),
+              "depth": torch.empty((H, W), dtype=torch.float32, device=dev)} for _ in range(B)]
+    for i, ((l, r), o) in enumerate(zip(raw, bouts)):
+        batch.bind(i, l, r, o)
+    batch.profile(True)
+    for _ in range(args.warmup):
+        batch.run(stream=stream)
+    barrier()
+    for o, bo in zip(outs, bouts):  # the batched results equal the per-frame ones
+        if not (torch.equal(o["disparity_u16"], bo["disparity_u16"]) and torch.equal(o["depth"], bo["depth"])):
+            raise SystemExit("batched and per-frame outputs differ")
+    launches0 = kernel_launches()
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        batch.run(stream=stream)
+    e1.record(stream)
+    barrier()
+    launches = batch.launches_per_run * args.steps  # graph replays launch the captured kernels
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    bstage = batch.stage_ms()
+    frames_total = B * args.steps * world
+    value = frames_total * PX_D / (ms * 1e-3) / 1e9
+
+    # ---- end to end through the public API: pinned host buffers, H2D inputs, batch, D2H results ------------
     host_in = [(torch.from_numpy(p.left).pin_memory(), torch.from_numpy(p.right).pin_memory()) for p in pairs]
-    host_out = [StereoResult(None, None, torch.empty((H, W), dtype=torch.int16).pin_memory().numpy().view(np.uint16),
-                             torch.empty((H, W), dtype=torch.float32).pin_memory().numpy()) for _ in range(B)]
-    host_np = [(a.numpy(), b.numpy()) for a, b in host_in]
+    host_out = [(torch.empty((H, W), dtype=torch.int16).pin_memory(), torch.empty((H, W), dtype=torch.float32).pin_memory())
+                for _ in range(B)]
 
     def e2e_step():
-        for (l, r), o in zip(host_np, host_out):
-            s.compute_raw(l, r, out=o)
+        for (hl, hr), (l, r) in zip(host_in, raw):
+            l.copy_(hl, non_blocking=True)
+            r.copy_(hr, non_blocking=True)
+        batch.run(stream=stream)
+        for (hu, hd), o in zip(host_out, bouts):
+            hu.copy_(o["disparity_u16"], non_blocking=True)
+            hd.copy_(o["depth"], non_blocking=True)
+        stream.synchronize()
 
     e2e_step()
     barrier()
+    e2e_steps = max(2, args.steps // 2)
     t0 = time.perf_counter()
-    e2e_steps = max(1, args.steps // 2)
     for _ in range(e2e_steps):
         e2e_step()
     barrier()
-    e2e_s = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
-    if world > 1:
-        torch.distributed.all_reduce(e2e_s, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = B * e2e_steps * world * PX_D / float(e2e_s.item()) / 1e9
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = B * e2e_steps * world * PX_D / e2e_s / 1e9
     clk.__exit__(None, None, None)
 
-    # ---- roofline of the dominant kernel --------------------------------------------------------------
-    stage_mean = stages.mean(axis=0) if len(stages) else np.zeros(5)
-    frame_tot = stages.sum(axis=1) if len(stages) else np.zeros(1)
-    dom = int(np.argmax(stage_mean))
+    # ---- roofline of the dominant kernel (batched SGM path launch) ---------------------------------------
     hbm, hbm_kind = peaks()
-    path_bytes = path_stage_bytes(W, H, D, P)
-    achieved = path_bytes / (stage_mean[2] * 1e-3) / 1e9 if stage_mean[2] > 0 else 0.0
+    path_bytes = path_stage_bytes(W, H, D, P) * B
+    paths_ms = float(bstage[3])
+    achieved = path_bytes / (paths_ms * 1e-3) / 1e9 if paths_ms > 0 else 0.0
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "paths_traffic.json")) as f:
-            traffic = json.load(f).get("dram_bytes_per_launch")
+            traffic = json.load(f).get("dram_bytes_per_launch_per_frame")
+            traffic = traffic * B if traffic else None
     except Exception:
         pass
-    roofline = {"bound": "hbm", "kernel": "k_paths (SGM path aggregation, 4 directions, one launch per frame)",
-                "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                "peak_kind": f"{hbm_kind} hbm_gbs", "traffic": traffic,
-                "algorithmic_bytes_per_launch": path_bytes, "kernel_ms": float(stage_mean[2]),
-                "share_of_frame": float(stage_mean[2] / max(stage_mean.sum(), 1e-9)),
-                "dominant_stage": STAGE_NAMES[dom],
-                "stage_ms": {n: float(v) for n, v in zip(STAGE_NAMES, stage_mean)},
+    roofline = {"bound": "hbm", "kernel": f"kb_paths (persistent SGM path aggregation, 4 directions, {B} frames per launch)",
+                "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_kind": f"{hbm_kind} hbm_gbs",
+                "traffic": traffic, "algorithmic_bytes_per_launch": path_bytes, "kernel_ms": paths_ms,
+                "share_of_step": paths_ms / max(float(bstage.sum()), 1e-9),
+                "stage_ms": {n: float(v) for n, v in zip(BATCH_STAGE_NAMES, bstage)},
                 "pipeline_formula_bytes_per_frame": algorithmic_bytes(W, H, D, P),
-                "pipeline_frac": algorithmic_bytes(W, H, D, P) / (float(np.median(frame_tot)) * 1e-3) / 1e9 / hbm}
+                "pipeline_frac": algorithmic_bytes(W, H, D, P) * B / (ms / args.steps * 1e-3) / 1e9 / hbm}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -323,20 +357,26 @@ def main():
     h2d = B * 2 * W * H
     d2h = B * W * H * (2 + 4)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "frames_per_step": B, "path": "per-frame launches",
+            "config": {"workload": WORKLOAD, "frames_per_step": B,
+                       "path": "batched: persistent launches per stage over all frames, one CUDA graph replay per step",
                        "kernel_config": s.kernel_config(),
-                       "l2": "working set per frame (671 MB of path values) far above the 126 MB L2",
+                       "l2": "working set per frame (~0.84 GB of cost and path volumes) far above the 126 MB L2",
                        "parallelism": f"replicas x{world}"},
+            "per_frame": {"value": per_frame_value, "unit": UNIT, "ms_per_frame": pf_ms / (args.steps * B),
+                          "frame_ms": {"p50": float(np.percentile(frame_tot, 50)), "p99": float(np.percentile(frame_tot, 99))},
+                          "stage_ms": {n: float(v) for n, v in zip(STAGE_NAMES, stages.mean(axis=0))} if len(stages) else {}},
+            "batched_over_per_frame": value / per_frame_value,
             "frame_ms": {"p50": float(np.percentile(frame_tot, 50)), "p99": float(np.percentile(frame_tot, 99)),
-                         "mean": float(frame_tot.mean())},
+                         "batch_latency_ms": ms / args.steps},
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "api": "CudaStereo.compute_raw (ds_compute_raw), pinned host buffers"},
+                    "api": "StereoBatch.run (ds_batch_run) with pinned host buffers copied in and results copied out"},
             "gpu_launches": int(launches), "clocks": clk.summary()}
     if rank == 0:
         print(json.dumps(line), flush=True)
+    batch.close()
     s.close()
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -186,6 +186,59 @@ typedef struct ds_kernel_config {
 DS_API int ds_set_kernel_config(ds_handle* handle, const ds_kernel_config* config);
 DS_API int ds_get_kernel_config(const ds_handle* handle, ds_kernel_config* config);
 
+/* ---- Batched path (no counterpart in the reference, which processes one frame per call) ----------
+ * Many pairs of uneven size and disparity range run together: every stage is one persistent launch
+ * per kernel variant that walks the blocks of all its pairs, and the whole batch is captured once into
+ * a CUDA graph that ds_batch_run replays. Results are identical to per-pair ds_compute* calls. */
+typedef struct ds_pair_desc {
+    int width, height;         /* stereo resolution */
+    ds_stereo_params params;
+    int raw;                   /* 1: inputs are raw and rectified with calibration `calib` */
+    int calib;                 /* 0 .. n_calib-1 */
+    int have_geometry;         /* 1: depth output with `geometry` and the depth gates */
+    ds_geometry geometry;
+    float min_depth_mm, max_depth_mm;
+    ds_kernel_config kernel;   /* regs_per_lane 0: the library's default; fused_pairs is ignored */
+} ds_pair_desc;
+
+typedef struct ds_batch ds_batch;
+
+/* Scheduling of a batch: pairs (heaviest first) are cut into micro-batches of `micro_batch` pairs that go
+ * through all stages back to back (so a pair's volumes are consumed while still in L2), and the
+ * micro-batches run round-robin on `branches` parallel branches of the graph. 0 = defaults (1, 4). */
+typedef struct ds_batch_options {
+    int micro_batch;
+    int branches;
+} ds_batch_options;
+
+DS_API int ds_batch_create(const ds_pair_desc* pairs, int n, int n_calib, const ds_batch_options* options,
+                           ds_batch** out);
+DS_API void ds_batch_destroy(ds_batch* batch);
+DS_API const char* ds_batch_last_error(const ds_batch* batch);
+/* Resident remap tables of calibration `calib` (as ds_set_rectification; tables of every raw pair using
+ * it must be at its stereo resolution or twice it). */
+DS_API int ds_batch_set_rectification(ds_batch* batch, int calib, const float* map_left_x, const float* map_left_y,
+                                      const float* map_right_x, const float* map_right_y, int map_width,
+                                      int map_height, int raw_width, int raw_height);
+/* Device pointers of pair `pair`: inputs (raw or rectified, tightly packed) and outputs (NULL entries
+ * go to the batch's internal buffers). Re-binding does not re-capture the graph. */
+DS_API int ds_batch_bind(ds_batch* batch, int pair, const uint8_t* left, const uint8_t* right, const ds_outputs* out);
+/* Enqueues the whole batch on `stream` (NULL: the batch's own stream) as one CUDA graph launch; the
+ * graph is captured on the first call. */
+DS_API int ds_batch_run(ds_batch* batch, void* stream);
+/* The same launches without a graph (for comparison and debugging). */
+DS_API int ds_batch_run_eager(ds_batch* batch, void* stream);
+DS_API size_t ds_batch_device_bytes(const ds_batch* batch);
+/* Kernel launches per run (persistent launches: one per stage and kernel variant). */
+DS_API int ds_batch_launches_per_run(const ds_batch* batch);
+/* Stage timing of the last run, measured on the first micro-batch (CUDA events captured into the graph
+ * between its stages, while the other branches run beside it):
+ * 0 rectify, 1 census, 2 costs, 3 SGM paths, 4 WTA + L-R, 5 median + outputs (DS_BATCH_STAGES).
+ * Enabling or disabling it captures the graph again on the next run. */
+#define DS_BATCH_STAGES 6
+DS_API int ds_batch_profile(ds_batch* batch, int on);
+DS_API int ds_batch_stage_ms(ds_batch* batch, double* ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,3 +17,4 @@ from .stereo import (  # noqa: F401
     StereoTimings,
     valid_disparity,
 )
+from .batch import PairDesc, StereoBatch  # noqa: F401,E402

@@ -49,6 +49,16 @@ class KernelConfigC(C.Structure):
                 ("fused_pairs", C.c_int), ("horz_warps_per_block", C.c_int)]
 
 
+class PairDescC(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("params", StereoParamsC), ("raw", C.c_int), ("calib", C.c_int),
+                ("have_geometry", C.c_int), ("geometry", GeometryC), ("min_depth_mm", C.c_float),
+                ("max_depth_mm", C.c_float), ("kernel", KernelConfigC)]
+
+
+class BatchOptionsC(C.Structure):
+    _fields_ = [("micro_batch", C.c_int), ("branches", C.c_int)]
+
+
 # Every symbol include/depth_cuda.h declares: name -> (restype, argtypes).
 _vp, _i, _f, _sz = C.c_void_p, C.c_int, C.c_float, C.c_size_t
 SIGNATURES = {
@@ -71,6 +81,17 @@ SIGNATURES = {
     "ds_kernel_launches": (C.c_uint64, []),
     "ds_set_kernel_config": (_i, [_vp, C.POINTER(KernelConfigC)]),
     "ds_get_kernel_config": (_i, [_vp, C.POINTER(KernelConfigC)]),
+    "ds_batch_create": (_i, [C.POINTER(PairDescC), _i, _i, C.POINTER(BatchOptionsC), C.POINTER(_vp)]),
+    "ds_batch_destroy": (None, [_vp]),
+    "ds_batch_last_error": (C.c_char_p, [_vp]),
+    "ds_batch_set_rectification": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _i, _i, _i, _i]),
+    "ds_batch_bind": (_i, [_vp, _i, _vp, _vp, C.POINTER(OutputsC)]),
+    "ds_batch_run": (_i, [_vp, _vp]),
+    "ds_batch_run_eager": (_i, [_vp, _vp]),
+    "ds_batch_device_bytes": (_sz, [_vp]),
+    "ds_batch_launches_per_run": (_i, [_vp]),
+    "ds_batch_profile": (_i, [_vp, _i]),
+    "ds_batch_stage_ms": (_i, [_vp, _vp]),
 }
 
 _lib = None

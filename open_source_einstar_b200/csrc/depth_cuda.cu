@@ -3,13 +3,17 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <algorithm>
 #include <chrono>
+#include <functional>
+#include <type_traits>
 #include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/depth_cuda.h"
+#include "batch_common.cuh"
 #include "dispatch.h"
 #include "frame_kernels.cuh"
 #include "fused_kernels.cuh"
@@ -66,12 +70,18 @@ struct ds_handle {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
-    uint8_t* d_rect[2] = {nullptr, nullptr};
+    uint8_t* d_rect[2] = {nullptr, nullptr};   // inside rect_raw, after kGuardRows guard rows
+    uint8_t* rect_raw[2] = {nullptr, nullptr};
     uint8_t* d_raw[2] = {nullptr, nullptr};
     float* d_map[4] = {nullptr, nullptr, nullptr, nullptr};  // lx, ly, rx, ry
     int map_w = 0, map_h = 0, raw_w = 0, raw_h = 0;
     bool have_rect = false;
-    void* d_census[2] = {nullptr, nullptr};
+    void* d_census[2] = {nullptr, nullptr};    // padded census: (y, x) at y * cpitch + x, inside census_raw
+    void* census_raw[2] = {nullptr, nullptr};
+    int cpitch = 0, cguard = 0;
+    size_t census_bytes = 0;                   // per image, guards included
+    void* d_S = nullptr;                       // fused pairs: vertical sums and horizontal scratch, inside d_values
+    void* d_T = nullptr;
     void* d_values = nullptr;
     size_t dir_stride = 0;
     size_t values_bytes = 0;
@@ -116,10 +126,10 @@ void release(ds_handle* h) {
     auto f = [](void* p) {
         if (p) cudaFree(p);
     };
-    for (auto* p : h->d_rect) f(p);
+    for (auto* p : h->rect_raw) f(p);
     for (auto* p : h->d_raw) f(p);
     for (auto* p : h->d_map) f(p);
-    for (auto* p : h->d_census) f(p);
+    for (auto* p : h->census_raw) f(p);
     f(h->d_values);
     f(h->d_costs);
     f(h->d_disp_lr);
@@ -171,7 +181,7 @@ int validate(const ds_stereo_params& p, int w, int h, std::string& msg) {
 constexpr size_t kMaxSmem = 227 * 1024;
 
 size_t horz_smem(const ds_handle* h, const ds::KernelCfg& c) {
-    return static_cast<size_t>(c.horz_warps) * (32 / c.seg) * h->w * 8;
+    return static_cast<size_t>(c.horz_warps) * (32 / c.seg) * h->w * 4 * dsk::kHorzWordsPerPixel;
 }
 
 dsk::FusedArgs fused_args(const ds_handle* h) {
@@ -179,9 +189,10 @@ dsk::FusedArgs fused_args(const ds_handle* h) {
     dsk::FusedArgs a{};
     a.census_l = h->d_census[0];
     a.census_r = h->d_census[1];
+    a.cpitch = h->cpitch;
     a.guide = h->d_rect[0];
-    a.S = h->d_values;
-    a.T = static_cast<uint8_t*>(h->d_values) + h->dir_stride * (h->s16 ? 2 : 1);
+    a.S = h->d_S;
+    a.T = h->d_T;
     a.w = h->w;
     a.h = h->h;
     a.nd = h->nd;
@@ -190,7 +201,10 @@ dsk::FusedArgs fused_args(const ds_handle* h) {
     a.p1 = sg.p1;
     a.invalid_cost = (2 * sg.census_radius_x + 1) * (2 * sg.census_radius_y + 1);
     a.slant = sg.slant_steps ? 1 : 0;
-    for (int q = 0; q < 32; ++q) a.p2_table[q] = sg.adaptive_p2 ? std::max(sg.p1 + 1, sg.p2 / (q + 1)) : sg.p2;
+    for (int q = 0; q < 32; ++q) {
+        const int p2 = sg.adaptive_p2 ? std::max(sg.p1 + 1, sg.p2 / (q + 1)) : sg.p2;
+        a.p2_table2[q] = static_cast<uint32_t>(p2) * 0x00010001u;
+    }
     a.uniqueness = sg.uniqueness;
     a.subpixel = h->p.subpixel ? 1 : 0;
     a.lr_max_diff = sg.lr_max_diff;
@@ -207,13 +221,15 @@ void launch_paths(ds_handle* h, cudaStream_t st) {
     const auto& sg = h->p.sgm;
     const int window = (2 * sg.census_radius_x + 1) * (2 * sg.census_radius_y + 1);
     if (h->cfg.materialize) {
-        dsk::CostArgs c{h->d_census[0], h->d_census[1], h->d_costs, h->w, h->h, h->nd, h->dp, sg.min_disparity, window};
+        dsk::CostArgs c{h->d_census[0], h->d_census[1], h->d_costs, h->w, h->h, h->nd, h->dp, sg.min_disparity, window,
+                        h->cpitch};
         DS_CUDA(ds::launch_costs(h->cfg, h->census64, c, st));
         ++g_launches;
     }
     dsk::PathArgs a{};
     a.census_l = h->d_census[0];
     a.census_r = h->d_census[1];
+    a.cpitch = h->cpitch;
     a.guide = h->d_rect[0];
     a.costs = h->cfg.materialize ? h->d_costs : nullptr;
     a.values = h->d_values;
@@ -256,12 +272,40 @@ void launch_wta(ds_handle* h, cudaStream_t st) {
     ++g_launches;
 }
 
-// (Re)allocates the buffers whose size depends on the kernel configuration.
+void free_counted(ds_handle* h, void*& p, size_t bytes) {
+    if (p) {
+        cudaFree(p);
+        h->bytes -= bytes;
+        p = nullptr;
+    }
+}
+
+// (Re)allocates the buffers whose size depends on the kernel configuration. The census and the fused
+// slabs carry kGuardRows guard rows above and below (and the census guard columns) for the prefetches.
 void size_config_buffers(ds_handle* h) {
+    constexpr int g = dsk::kGuardRows;
     h->dp = h->cfg.dp();
     const size_t n = static_cast<size_t>(h->w) * h->h;
     h->dir_stride = n * static_cast<size_t>(h->dp);
-    const size_t vb = h->cfg.fused ? h->dir_stride * 2 * (h->s16 ? 2 : 1) : h->dir_stride * h->ndirs * (h->wide ? 2 : 1);
+    {
+        const int mind = h->p.sgm.min_disparity;
+        const int guard = (std::max(mind + h->dp, 0) + std::max(-mind, 0) + g + 4 + 3) / 4 * 4;
+        const int pitch = (h->w + 2 * guard + 3) / 4 * 4;
+        const size_t cw = h->census64 ? 8 : 4;
+        const size_t cb = static_cast<size_t>(h->h + 2 * g) * pitch * cw;
+        if (cb != h->census_bytes) {
+            for (auto*& p : h->census_raw) free_counted(h, p, h->census_bytes);
+            h->census_bytes = 0;
+            for (auto*& p : h->census_raw) p = h->alloc<uint8_t>(cb);
+            h->census_bytes = cb;
+        }
+        h->cguard = guard;
+        h->cpitch = pitch;
+        for (int s = 0; s < 2; ++s)
+            h->d_census[s] = static_cast<uint8_t*>(h->census_raw[s]) + (static_cast<size_t>(g) * pitch + guard) * cw;
+    }
+    const size_t slab = static_cast<size_t>(h->h + 2 * g) * h->w * h->dp * (h->s16 ? 2 : 1);  // fused, bytes
+    const size_t vb = h->cfg.fused ? 2 * slab : h->dir_stride * h->ndirs * (h->wide ? 2 : 1);
     if (vb != h->values_bytes) {
         if (h->d_values) {
             cudaFree(h->d_values);
@@ -271,6 +315,13 @@ void size_config_buffers(ds_handle* h) {
         }
         h->d_values = h->alloc<uint8_t>(vb);
         h->values_bytes = vb;
+    }
+    if (h->cfg.fused) {
+        const size_t lead = static_cast<size_t>(g) * h->w * h->dp * (h->s16 ? 2 : 1);
+        h->d_S = static_cast<uint8_t*>(h->d_values) + lead;
+        h->d_T = static_cast<uint8_t*>(h->d_values) + slab + lead;
+    } else {
+        h->d_S = h->d_T = nullptr;
     }
     const size_t cb = h->cfg.materialize && !h->cfg.fused ? n * static_cast<size_t>(h->dp) : 0;
     if (cb != h->costs_bytes) {
@@ -342,6 +393,7 @@ void enqueue_frame(ds_handle* h, const uint8_t* left, const uint8_t* right, bool
         c.h = h->h;
         c.rx = h->p.sgm.census_radius_x;
         c.ry = h->p.sgm.census_radius_y;
+        c.pitch = h->cpitch;
         dim3 b(32, 8), g((h->w + 31) / 32, (h->h + 7) / 8, 2);
         if (h->census64) dsk::k_census<uint64_t><<<g, b, 0, st>>>(c);
         else dsk::k_census<uint32_t><<<g, b, 0, st>>>(c);
@@ -469,9 +521,84 @@ cudaError_t launch_vert(const KernelCfg& cfg, bool c64, bool s16, const dsk::Fus
 cudaError_t launch_horz(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, size_t smem, cudaStream_t st) {
     DS_BY_R(launch_horz, cfg, c64, s16, a, smem, st)
 }
+cudaError_t launch_paths_batch(const KernelCfg& cfg, bool c64, bool wide, const dsk::PathArgs* args, const BatchGroupDev& g,
+                               cudaStream_t st) {
+    DS_BY_R(launch_paths_batch, cfg, c64, wide, args, g, st)
+}
+cudaError_t launch_wta_batch(const KernelCfg& cfg, bool wide, int ndirs, const dsk::WtaArgs* args, const BatchGroupDev& g,
+                             size_t smem, cudaStream_t st) {
+    DS_BY_R(launch_wta_batch, cfg, wide, ndirs, args, g, smem, st)
+}
+cudaError_t launch_costs_batch(const KernelCfg& cfg, bool c64, const dsk::CostArgs* args, const BatchGroupDev& g,
+                               cudaStream_t st) {
+    DS_BY_R(launch_costs_batch, cfg, c64, args, g, st)
+}
 #undef DS_BY_R
 
 }  // namespace ds
+
+namespace dsk {
+
+// Persistent batch launches of the per-pixel stages; per group pair i: grid gx[i] x gy[i] x (2 or 1).
+__device__ __forceinline__ void decode3(int lb, int gx, int gy, int& bx, int& by, int& bz) {
+    bx = lb % gx;
+    const int t = lb / gx;
+    by = t % gy;
+    bz = t / gy;
+}
+
+// Block-uniform staging of a pair's arguments in shared memory (all threads call it).
+template <typename A>
+__device__ __forceinline__ void stage_args(A& sa, const A* args, int p, int& cur) {
+    if (p != cur) {
+        __syncthreads();
+        if (threadIdx.x == 0 && threadIdx.y == 0) sa = args[p];
+        __syncthreads();
+        cur = p;
+    }
+}
+
+__global__ void kb_rectify(const RectifyArgs* __restrict__ args, const int* __restrict__ pairs, const int* __restrict__ prefix,
+                           const int* __restrict__ gx, const int* __restrict__ gy, int n, int total) {
+    __shared__ RectifyArgs sa;
+    int cur = -1;
+    for (int v = blockIdx.x; v < total; v += gridDim.x) {
+        const int i = batch_find(prefix, n, v);
+        int bx, by, bz;
+        decode3(v - __ldg(prefix + i), __ldg(gx + i), __ldg(gy + i), bx, by, bz);
+        stage_args(sa, args, __ldg(pairs + i), cur);
+        rectify_body(sa, bx, by, bz);
+    }
+}
+
+template <typename W>
+__global__ void kb_census(const CensusArgs* __restrict__ args, const int* __restrict__ pairs, const int* __restrict__ prefix,
+                          const int* __restrict__ gx, const int* __restrict__ gy, int n, int total) {
+    __shared__ CensusArgs sa;
+    int cur = -1;
+    for (int v = blockIdx.x; v < total; v += gridDim.x) {
+        const int i = batch_find(prefix, n, v);
+        int bx, by, bz;
+        decode3(v - __ldg(prefix + i), __ldg(gx + i), __ldg(gy + i), bx, by, bz);
+        stage_args(sa, args, __ldg(pairs + i), cur);
+        census_body<W>(sa, bx, by, bz);
+    }
+}
+
+__global__ void kb_post(const PostArgs* __restrict__ args, const int* __restrict__ pairs, const int* __restrict__ prefix,
+                        const int* __restrict__ gx, const int* __restrict__ gy, int n, int total) {
+    __shared__ PostArgs sa;
+    int cur = -1;
+    for (int v = blockIdx.x; v < total; v += gridDim.x) {
+        const int i = batch_find(prefix, n, v);
+        int bx, by, bz;
+        decode3(v - __ldg(prefix + i), __ldg(gx + i), __ldg(gy + i), bx, by, bz);
+        stage_args(sa, args, __ldg(pairs + i), cur);
+        post_body(sa, bx, by);
+    }
+}
+
+}  // namespace dsk
 
 extern "C" {
 
@@ -526,18 +653,17 @@ DS_API int ds_create(const ds_stereo_params* params, int width, int height, ds_h
         h->s16 = h->wide || 2 * (window + params->sgm.p2) > 255;
         h->cfg.fused = false;  // the fused pairs are selectable (ds_set_kernel_config / autotuner)
         if (h->ndirs == 4) {
-            const int rows_max = static_cast<int>(kMaxSmem / (static_cast<size_t>(width) * 8));
+            const int rows_max = static_cast<int>(kMaxSmem / (static_cast<size_t>(width) * 4 * dsk::kHorzWordsPerPixel));
             h->cfg.horz_warps = std::max(1, std::min(4, rows_max / (32 / h->cfg.seg)));
         }
         DS_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
         DS_CUDA(cudaEventCreate(&h->ev0));
         DS_CUDA(cudaEventCreate(&h->ev1));
         const size_t n = static_cast<size_t>(width) * height;
-        h->d_rect[0] = h->alloc<uint8_t>(n);
-        h->d_rect[1] = h->alloc<uint8_t>(n);
-        const size_t cw = h->census64 ? 8 : 4;
-        h->d_census[0] = h->alloc<uint8_t>(n * cw);
-        h->d_census[1] = h->alloc<uint8_t>(n * cw);
+        for (int s = 0; s < 2; ++s) {
+            h->rect_raw[s] = h->alloc<uint8_t>(n + 2 * static_cast<size_t>(dsk::kGuardRows) * width);
+            h->d_rect[s] = h->rect_raw[s] + static_cast<size_t>(dsk::kGuardRows) * width;
+        }
         size_config_buffers(h);
         h->d_disp_lr = h->alloc<float>(n);
         h->d_out_disp = h->alloc<float>(n);
@@ -668,12 +794,16 @@ DS_API int ds_debug_read(ds_handle* h, uint64_t* census_left, uint64_t* census_r
         uint64_t* dst[2] = {census_left, census_right};
         for (int s = 0; s < 2; ++s) {
             if (!dst[s]) continue;
-            if (h->census64) {
-                DS_CUDA(cudaMemcpy(dst[s], h->d_census[s], n * 8, cudaMemcpyDeviceToHost));
-            } else {
-                std::vector<uint32_t> tmp(n);
-                DS_CUDA(cudaMemcpy(tmp.data(), h->d_census[s], n * 4, cudaMemcpyDeviceToHost));
-                for (size_t i = 0; i < n; ++i) dst[s][i] = tmp[i];
+            const size_t cw = h->census64 ? 8 : 4;
+            std::vector<uint8_t> tmp(n * cw);
+            DS_CUDA(cudaMemcpy2D(tmp.data(), h->w * cw, h->d_census[s], h->cpitch * cw, h->w * cw, h->h, cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < n; ++i) {
+                if (h->census64) std::memcpy(&dst[s][i], &tmp[i * 8], 8);
+                else {
+                    uint32_t v;
+                    std::memcpy(&v, &tmp[i * 4], 4);
+                    dst[s][i] = v;
+                }
             }
         }
         if (path_sums) {
@@ -694,6 +824,7 @@ DS_API int ds_debug_read(ds_handle* h, uint64_t* census_left, uint64_t* census_r
                     dsk::PathArgs pa{};
                     pa.census_l = h->d_census[0];
                     pa.census_r = h->d_census[1];
+                    pa.cpitch = h->cpitch;
                     pa.guide = h->d_rect[0];
                     pa.values = tmp;
                     pa.dir_stride = h->dir_stride;
@@ -810,6 +941,617 @@ DS_API int ds_get_kernel_config(const ds_handle* h, ds_kernel_config* c) {
     c->fused_pairs = h->cfg.fused ? 1 : 0;
     c->horz_warps_per_block = h->cfg.horz_warps;
     return DS_OK;
+}
+
+}  // extern "C"
+
+// ================================================================================================
+// Batched path: many pairs of uneven size / disparity range in one persistent launch per stage and
+// kernel variant, captured once into a CUDA graph and replayed.
+
+namespace {
+
+template <typename T>
+T* dev_upload(const std::vector<T>& v) {
+    T* d = nullptr;
+    if (v.empty()) return nullptr;
+    DS_CUDA(cudaMalloc(&d, v.size() * sizeof(T)));
+    DS_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return d;
+}
+
+struct BatchGroup {
+    ds::KernelCfg cfg;
+    bool c64 = false, wide = false;
+    int ndirs = 4;
+    size_t smem = 0;
+    std::vector<int> pairs, prefix, gx, gy;
+    int total = 0;
+    int *d_pairs = nullptr, *d_prefix = nullptr, *d_gx = nullptr, *d_gy = nullptr;
+    ds::BatchGroupDev dev() const { return {d_pairs, d_prefix, d_gx, static_cast<int>(pairs.size()), total, 0}; }
+    void upload() {
+        std::vector<int> pre = prefix;
+        pre.push_back(total);
+        d_pairs = dev_upload(pairs);
+        d_prefix = dev_upload(pre);
+        d_gx = dev_upload(gx);
+        d_gy = dev_upload(gy);
+    }
+    void release() {
+        for (int* p : {d_pairs, d_prefix, d_gx, d_gy})
+            if (p) cudaFree(p);
+        d_pairs = d_prefix = d_gx = d_gy = nullptr;
+    }
+};
+
+struct BatchCalib {
+    float* map[4] = {nullptr, nullptr, nullptr, nullptr};
+    int map_w = 0, map_h = 0, raw_w = 0, raw_h = 0;
+};
+
+}  // namespace
+
+struct ds_batch {
+    std::vector<ds_pair_desc> desc;
+    std::vector<ds_handle*> h;
+    std::vector<BatchCalib> calib;
+    std::vector<const uint8_t*> in_l, in_r;
+    std::vector<ds_outputs> out;
+    // per-pair stage arguments (host mirrors and device arrays)
+    std::vector<dsk::RectifyArgs> a_rect;
+    std::vector<dsk::CensusArgs> a_census;
+    std::vector<dsk::CostArgs> a_costs;
+    std::vector<dsk::PathArgs> a_paths;
+    std::vector<dsk::WtaArgs> a_wta;
+    std::vector<dsk::PostArgs> a_post;
+    dsk::RectifyArgs* d_rect = nullptr;
+    dsk::CensusArgs* d_census = nullptr;
+    dsk::CostArgs* d_costs = nullptr;
+    dsk::PathArgs* d_paths = nullptr;
+    dsk::WtaArgs* d_wta = nullptr;
+    dsk::PostArgs* d_post = nullptr;
+    struct Micro {
+        BatchGroup g_rect, g_post;
+        std::vector<BatchGroup> g_census, g_costs, g_paths, g_wta;
+        int launches() const {
+            return (g_rect.total > 0 ? 1 : 0) + static_cast<int>(g_census.size() + g_costs.size() + g_paths.size() + g_wta.size()) + 1;
+        }
+    };
+    std::vector<Micro> micro;  // pairs in micro-batches run through all stages back to back
+    int micro_batch = 1, branches = 4;  // best measured for 1280x1024, D=128 on B200
+    std::vector<cudaStream_t> branch_st;
+    std::vector<cudaEvent_t> fork_join;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool args_dirty = true;
+    bool profile = false;
+    cudaEvent_t ev[DS_BATCH_STAGES + 1] = {};
+    std::string err;
+    size_t bytes = 0;
+    int fail(int code, std::string m) {
+        err = std::move(m);
+        return code;
+    }
+};
+
+namespace {
+
+void batch_release(ds_batch* b) {
+    if (!b) return;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (auto e : b->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto* h : b->h) {
+        if (!h) continue;
+        for (auto*& p : h->d_map) p = nullptr;  // the maps belong to the batch's calibrations
+        release(h);
+        delete h;
+    }
+    for (auto& c : b->calib)
+        for (auto* p : c.map)
+            if (p) cudaFree(p);
+    for (void* p : {static_cast<void*>(b->d_rect), static_cast<void*>(b->d_census), static_cast<void*>(b->d_costs),
+                    static_cast<void*>(b->d_paths), static_cast<void*>(b->d_wta), static_cast<void*>(b->d_post)})
+        if (p) cudaFree(p);
+    for (auto& m : b->micro) {
+        m.g_rect.release();
+        m.g_post.release();
+        for (auto* gs : {&m.g_census, &m.g_costs, &m.g_paths, &m.g_wta})
+            for (auto& g : *gs) g.release();
+    }
+    for (auto s : b->branch_st)
+        if (s) cudaStreamDestroy(s);
+    for (auto e : b->fork_join)
+        if (e) cudaEventDestroy(e);
+    if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+// Per-pair stage arguments from the pair's handle and current bindings.
+void batch_fill_args(ds_batch* b) {
+    const int n = static_cast<int>(b->h.size());
+    b->a_rect.assign(n, {});
+    b->a_census.assign(n, {});
+    b->a_costs.assign(n, {});
+    b->a_paths.assign(n, {});
+    b->a_wta.assign(n, {});
+    b->a_post.assign(n, {});
+    for (int i = 0; i < n; ++i) {
+        ds_handle* h = b->h[i];
+        const ds_pair_desc& d = b->desc[i];
+        const auto& sg = h->p.sgm;
+        const int window = (2 * sg.census_radius_x + 1) * (2 * sg.census_radius_y + 1);
+        const uint8_t* img[2] = {b->in_l[i], b->in_r[i]};
+        if (d.raw) {
+            const BatchCalib& c = b->calib[d.calib];
+            auto& r = b->a_rect[i];
+            for (int s = 0; s < 2; ++s) {
+                r.raw[s] = img[s];
+                r.map_x[s] = c.map[2 * s];
+                r.map_y[s] = c.map[2 * s + 1];
+                r.out[s] = h->d_rect[s];
+            }
+            r.raw_w = c.raw_w;
+            r.raw_h = c.raw_h;
+            r.map_w = c.map_w;
+            r.out_w = h->w;
+            r.out_h = h->h;
+            r.half = c.map_w == 2 * h->w ? 1 : 0;
+            img[0] = h->d_rect[0];
+            img[1] = h->d_rect[1];
+        }
+        auto& ce = b->a_census[i];
+        ce.img[0] = img[0];
+        ce.img[1] = img[1];
+        ce.out[0] = h->d_census[0];
+        ce.out[1] = h->d_census[1];
+        ce.w = h->w;
+        ce.h = h->h;
+        ce.rx = sg.census_radius_x;
+        ce.ry = sg.census_radius_y;
+        ce.pitch = h->cpitch;
+        b->a_costs[i] = dsk::CostArgs{h->d_census[0], h->d_census[1], h->d_costs, h->w, h->h, h->nd, h->dp, sg.min_disparity,
+                                      window, h->cpitch};
+        auto& pa = b->a_paths[i];
+        pa.census_l = h->d_census[0];
+        pa.census_r = h->d_census[1];
+        pa.cpitch = h->cpitch;
+        pa.guide = img[0];
+        pa.costs = h->cfg.materialize ? h->d_costs : nullptr;
+        pa.values = h->d_values;
+        pa.dir_stride = h->dir_stride;
+        pa.w = h->w;
+        pa.h = h->h;
+        pa.nd = h->nd;
+        pa.dp = h->dp;
+        pa.min_disp = sg.min_disparity;
+        pa.p1 = sg.p1;
+        pa.invalid_cost = window;
+        pa.slant = sg.slant_steps ? 1 : 0;
+        pa.dir_base = 0;
+        for (int q = 0; q < 32; ++q) pa.p2_table[q] = sg.adaptive_p2 ? std::max(sg.p1 + 1, sg.p2 / (q + 1)) : sg.p2;
+        auto& wa = b->a_wta[i];
+        wa.values = h->d_values;
+        wa.dir_stride = h->dir_stride;
+        wa.ndirs = h->ndirs;
+        wa.w = h->w;
+        wa.h = h->h;
+        wa.nd = h->nd;
+        wa.dp = h->dp;
+        wa.min_disp = sg.min_disparity;
+        wa.uniqueness = sg.uniqueness;
+        wa.subpixel = h->p.subpixel ? 1 : 0;
+        wa.lr_max_diff = sg.lr_max_diff;
+        wa.disp = h->d_disp_lr;
+        auto& q = b->a_post[i];
+        const ds_outputs& o = b->out[i];
+        q.disp = h->d_disp_lr;
+        q.w = h->w;
+        q.h = h->h;
+        q.median = h->p.median ? 1 : 0;
+        q.min_disp = sg.min_disparity;
+        q.out_disp = o.disparity ? o.disparity : h->d_out_disp;
+        q.out_conf = o.confidence;
+        q.out_u16 = o.disparity_u16 ? o.disparity_u16 : h->d_out_u16;
+        q.out_depth = d.have_geometry ? (o.depth ? o.depth : h->d_out_depth) : nullptr;
+        q.f = d.geometry.f;
+        q.baseline = d.geometry.baseline;
+        q.cx_offset = d.geometry.cx_offset;
+        q.min_depth = d.min_depth_mm;
+        q.max_depth = d.max_depth_mm;
+    }
+    auto put = [](auto& v, auto*& dst) {
+        using T = typename std::remove_reference_t<decltype(v)>::value_type;
+        if (!dst) DS_CUDA(cudaMalloc(&dst, v.size() * sizeof(T)));
+        DS_CUDA(cudaMemcpy(dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    };
+    put(b->a_rect, b->d_rect);
+    put(b->a_census, b->d_census);
+    put(b->a_costs, b->d_costs);
+    put(b->a_paths, b->d_paths);
+    put(b->a_wta, b->d_wta);
+    put(b->a_post, b->d_post);
+    b->args_dirty = false;
+}
+
+void batch_plan_micro(ds_batch* b, ds_batch::Micro& m, const std::vector<int>& order);
+
+// Splits the pairs (heaviest first) into micro-batches; within each, groups pairs by kernel variant and
+// lays out each group's virtual blocks.
+void batch_plan(ds_batch* b) {
+    const int n = static_cast<int>(b->h.size());
+    std::vector<int> all(n);
+    for (int i = 0; i < n; ++i) all[i] = i;
+    std::stable_sort(all.begin(), all.end(), [&](int x, int y) {
+        const ds_handle *a = b->h[x], *c = b->h[y];
+        return static_cast<double>(a->w) * a->h * a->nd > static_cast<double>(c->w) * c->h * c->nd;
+    });
+    const int mb = std::max(1, std::min(b->micro_batch, n));
+    for (int first = 0; first < n; first += mb) {
+        b->micro.emplace_back();
+        std::vector<int> order(all.begin() + first, all.begin() + std::min(n, first + mb));
+        batch_plan_micro(b, b->micro.back(), order);
+    }
+}
+
+void batch_plan_micro(ds_batch* b, ds_batch::Micro& m, const std::vector<int>& order) {
+    auto add = [](BatchGroup& g, int pair, int blocks, int gx, int gy) {
+        g.pairs.push_back(pair);
+        g.prefix.push_back(g.total);
+        g.gx.push_back(gx);
+        g.gy.push_back(gy);
+        g.total += blocks;
+    };
+    auto find_or_add = [](std::vector<BatchGroup>& gs, auto match) -> BatchGroup& {
+        for (auto& g : gs)
+            if (match(g)) return g;
+        gs.emplace_back();
+        return gs.back();
+    };
+    for (int i : order) {
+        ds_handle* h = b->h[i];
+        const int tx = (h->w + 31) / 32, ty = (h->h + 7) / 8;
+        if (b->desc[i].raw) add(m.g_rect, i, tx * ty * 2, tx, ty);
+        add(m.g_post, i, tx * ty, tx, ty);
+        {
+            BatchGroup& g = find_or_add(m.g_census, [&](const BatchGroup& x) { return x.c64 == h->census64; });
+            g.c64 = h->census64;
+            add(g, i, tx * ty * 2, tx, ty);
+        }
+        const ds::KernelCfg& c = h->cfg;
+        if (c.materialize) {
+            BatchGroup& g = find_or_add(m.g_costs, [&](const BatchGroup& x) {
+                return x.cfg.R == c.R && x.cfg.seg == c.seg && x.c64 == h->census64;
+            });
+            g.cfg = c;
+            g.c64 = h->census64;
+            const long px = static_cast<long>(h->w) * h->h, per = 8 * (32 / c.seg);
+            add(g, i, static_cast<int>((px + per - 1) / per), 1, 1);
+        }
+        {
+            BatchGroup& g = find_or_add(m.g_paths, [&](const BatchGroup& x) {
+                return x.cfg.R == c.R && x.cfg.seg == c.seg && x.cfg.materialize == c.materialize && x.cfg.prefetch == c.prefetch &&
+                       x.cfg.paths_warps == c.paths_warps && x.c64 == h->census64 && x.wide == h->wide;
+            });
+            g.cfg = c;
+            g.c64 = h->census64;
+            g.wide = h->wide;
+            const int max_lines = h->ndirs == 8 ? h->w + h->h - 1 : std::max(h->w, h->h);
+            const int lpb = c.paths_warps * (32 / c.seg);
+            const int gx = (max_lines + lpb - 1) / lpb;
+            add(g, i, gx * h->ndirs, gx, 1);
+        }
+        {
+            BatchGroup& g = find_or_add(m.g_wta, [&](const BatchGroup& x) {
+                return x.cfg.R == c.R && x.cfg.seg == c.seg && x.cfg.wta_threads == c.wta_threads && x.wide == h->wide &&
+                       x.ndirs == h->ndirs;
+            });
+            g.cfg = c;
+            g.wide = h->wide;
+            g.ndirs = h->ndirs;
+            g.smem = std::max(g.smem, static_cast<size_t>(h->w) * 8);
+            add(g, i, h->h, 1, 1);
+        }
+    }
+    m.g_rect.upload();
+    m.g_post.upload();
+    for (auto* gs : {&m.g_census, &m.g_costs, &m.g_paths, &m.g_wta})
+        for (auto& g : *gs) g.upload();
+}
+
+void batch_enqueue_micro(ds_batch* b, const ds_batch::Micro& m, cudaStream_t st, bool capturing, bool marks) {
+    using namespace dsk;
+    auto grid_of = [](auto k, int threads, size_t smem, int total) { return ds::persistent_grid(k, threads, smem, total); };
+    auto mark = [&](int i) {
+        // Inside a capture, only an external event record becomes a timestamped node of the graph.
+        if (marks) DS_CUDA(cudaEventRecordWithFlags(b->ev[i], st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault));
+    };
+    mark(0);
+    if (m.g_rect.total > 0) {
+        const auto& g = m.g_rect;
+        kb_rectify<<<grid_of(kb_rectify, 256, 0, g.total), dim3(32, 8), 0, st>>>(b->d_rect, g.d_pairs, g.d_prefix, g.d_gx, g.d_gy,
+                                                                                 static_cast<int>(g.pairs.size()), g.total);
+        ++g_launches;
+    }
+    mark(1);
+    for (const auto& g : m.g_census) {
+        if (g.c64)
+            kb_census<uint64_t><<<grid_of(kb_census<uint64_t>, 256, 0, g.total), dim3(32, 8), 0, st>>>(
+                b->d_census, g.d_pairs, g.d_prefix, g.d_gx, g.d_gy, static_cast<int>(g.pairs.size()), g.total);
+        else
+            kb_census<uint32_t><<<grid_of(kb_census<uint32_t>, 256, 0, g.total), dim3(32, 8), 0, st>>>(
+                b->d_census, g.d_pairs, g.d_prefix, g.d_gx, g.d_gy, static_cast<int>(g.pairs.size()), g.total);
+        ++g_launches;
+    }
+    mark(2);
+    for (const auto& g : m.g_costs) {
+        DS_CUDA(ds::launch_costs_batch(g.cfg, g.c64, b->d_costs, g.dev(), st));
+        ++g_launches;
+    }
+    mark(3);
+    for (const auto& g : m.g_paths) {
+        DS_CUDA(ds::launch_paths_batch(g.cfg, g.c64, g.wide, b->d_paths, g.dev(), st));
+        ++g_launches;
+    }
+    mark(4);
+    for (const auto& g : m.g_wta) {
+        DS_CUDA(ds::launch_wta_batch(g.cfg, g.wide, g.ndirs, b->d_wta, g.dev(), g.smem, st));
+        ++g_launches;
+    }
+    mark(5);
+    {
+        const auto& g = m.g_post;
+        kb_post<<<grid_of(kb_post, 256, 0, g.total), dim3(32, 8), 0, st>>>(b->d_post, g.d_pairs, g.d_prefix, g.d_gx, g.d_gy,
+                                                                          static_cast<int>(g.pairs.size()), g.total);
+        ++g_launches;
+    }
+    mark(6);
+    DS_CUDA(cudaGetLastError());
+}
+
+// All micro-batches: round-robin over `branches` streams forked from `st` and joined back into it.
+void batch_enqueue(ds_batch* b, cudaStream_t st, bool capturing) {
+    const int nb = std::max(1, std::min(b->branches, static_cast<int>(b->micro.size())));
+    if (nb == 1) {
+        for (size_t i = 0; i < b->micro.size(); ++i) batch_enqueue_micro(b, b->micro[i], st, capturing, b->profile && i == 0);
+        return;
+    }
+    DS_CUDA(cudaEventRecord(b->fork_join[0], st));
+    for (int k = 0; k < nb; ++k) {
+        DS_CUDA(cudaStreamWaitEvent(b->branch_st[k], b->fork_join[0], 0));
+        for (size_t i = k; i < b->micro.size(); i += nb)
+            batch_enqueue_micro(b, b->micro[i], b->branch_st[k], capturing, b->profile && i == 0);
+        DS_CUDA(cudaEventRecord(b->fork_join[1 + k], b->branch_st[k]));
+    }
+    for (int k = 0; k < nb; ++k) DS_CUDA(cudaStreamWaitEvent(st, b->fork_join[1 + k], 0));
+}
+
+int batch_guarded(ds_batch* b, const std::function<int()>& f) {
+    try {
+        return f();
+    } catch (const CudaFailure& e) {
+        std::string m = std::string("CUDA batch failed: ") + e.what + ": " + cudaGetErrorString(e.err);
+        if (b) b->err = m;
+        g_error = m;
+        return DS_IO;
+    } catch (const std::bad_alloc&) {
+        if (b) b->err = "host allocation failed";
+        g_error = "host allocation failed";
+        return DS_IO;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+DS_API int ds_batch_create(const ds_pair_desc* pairs, int n, int n_calib, const ds_batch_options* opt, ds_batch** out) {
+    if (!pairs || !out || n < 1 || n > 65536 || n_calib < 0) {
+        g_error = "invalid batch description";
+        return DS_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    auto* b = new (std::nothrow) ds_batch();
+    if (!b) {
+        g_error = "host allocation failed";
+        return DS_IO;
+    }
+    int rc = DS_OK;
+    for (int i = 0; i < n && rc == DS_OK; ++i) {
+        const ds_pair_desc& d = pairs[i];
+        if (d.raw && (d.calib < 0 || d.calib >= n_calib)) {
+            g_error = "pair " + std::to_string(i) + ": calibration index out of range";
+            rc = DS_INVALID_ARGUMENT;
+            break;
+        }
+        ds_handle* h = nullptr;
+        rc = ds_create(&d.params, d.width, d.height, &h);
+        if (rc != DS_OK) {
+            g_error = "pair " + std::to_string(i) + ": " + g_error;
+            break;
+        }
+        b->h.push_back(h);
+        if (d.kernel.regs_per_lane > 0) {
+            ds_kernel_config kc = d.kernel;
+            kc.fused_pairs = 0;  // the batched path runs the per-direction kernels
+            rc = ds_set_kernel_config(h, &kc);
+            if (rc != DS_OK) g_error = "pair " + std::to_string(i) + ": " + h->err;
+        } else if (h->cfg.fused) {
+            h->cfg.fused = false;
+            rc = batch_guarded(b, [&] {
+                size_config_buffers(h);
+                return DS_OK;
+            });
+        }
+    }
+    if (rc == DS_OK) {
+        rc = batch_guarded(b, [&]() -> int {
+            b->desc.assign(pairs, pairs + n);
+            b->calib.assign(n_calib, BatchCalib{});
+            b->in_l.assign(n, nullptr);
+            b->in_r.assign(n, nullptr);
+            b->out.assign(n, ds_outputs{});
+            for (auto* h : b->h) b->bytes += h->bytes;
+            if (opt) {
+                b->micro_batch = opt->micro_batch > 0 ? opt->micro_batch : b->micro_batch;
+                b->branches = opt->branches > 0 ? std::min(opt->branches, 16) : b->branches;
+            }
+            DS_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+            b->branch_st.assign(b->branches, nullptr);
+            for (auto& st : b->branch_st) DS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            b->fork_join.assign(b->branches + 1, nullptr);
+            for (auto& e : b->fork_join) DS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            batch_plan(b);
+            return DS_OK;
+        });
+    }
+    if (rc != DS_OK) {
+        std::string m = g_error;
+        batch_release(b);
+        delete b;
+        g_error = m;
+        return rc;
+    }
+    *out = b;
+    return DS_OK;
+}
+
+DS_API void ds_batch_destroy(ds_batch* b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_release(b);
+    delete b;
+}
+
+DS_API const char* ds_batch_last_error(const ds_batch* b) { return b ? b->err.c_str() : g_error.c_str(); }
+
+DS_API int ds_batch_set_rectification(ds_batch* b, int calib, const float* lx, const float* ly, const float* rx,
+                                      const float* ry, int map_w, int map_h, int raw_w, int raw_h) {
+    if (!b) return DS_INVALID_ARGUMENT;
+    if (calib < 0 || calib >= static_cast<int>(b->calib.size())) return b->fail(DS_INVALID_ARGUMENT, "calibration index out of range");
+    if (!lx || !ly || !rx || !ry) return b->fail(DS_INVALID_ARGUMENT, "null remap table");
+    if (raw_w < 2 || raw_h < 2 || raw_w > 16384 || raw_h > 16384) return b->fail(DS_INVALID_ARGUMENT, "raw size out of range");
+    for (size_t i = 0; i < b->h.size(); ++i) {
+        if (!b->desc[i].raw || b->desc[i].calib != calib) continue;
+        const ds_handle* h = b->h[i];
+        const bool same = map_w == h->w && map_h == h->h, twice = map_w == 2 * h->w && map_h == 2 * h->h;
+        if (!same && !twice) return b->fail(DS_INVALID_ARGUMENT, "remap resolution must be the stereo resolution or twice it");
+    }
+    return batch_guarded(b, [&]() -> int {
+        BatchCalib& c = b->calib[calib];
+        const size_t n = static_cast<size_t>(map_w) * map_h;
+        if (c.map_w != map_w || c.map_h != map_h) {
+            for (auto*& p : c.map) {
+                if (p) cudaFree(p), b->bytes -= static_cast<size_t>(c.map_w) * c.map_h * 4;
+                p = nullptr;
+            }
+            for (auto*& p : c.map) {
+                DS_CUDA(cudaMalloc(&p, n * 4));
+                b->bytes += n * 4;
+            }
+        }
+        const float* src[4] = {lx, ly, rx, ry};
+        for (int i = 0; i < 4; ++i) DS_CUDA(cudaMemcpy(c.map[i], src[i], n * 4, cudaMemcpyHostToDevice));
+        c.map_w = map_w;
+        c.map_h = map_h;
+        c.raw_w = raw_w;
+        c.raw_h = raw_h;
+        b->args_dirty = true;
+        return DS_OK;
+    });
+}
+
+DS_API int ds_batch_bind(ds_batch* b, int pair, const uint8_t* left, const uint8_t* right, const ds_outputs* out) {
+    if (!b) return DS_INVALID_ARGUMENT;
+    if (pair < 0 || pair >= static_cast<int>(b->h.size())) return b->fail(DS_INVALID_ARGUMENT, "pair index out of range");
+    if (!left || !right) return b->fail(DS_INVALID_ARGUMENT, "null image");
+    b->in_l[pair] = left;
+    b->in_r[pair] = right;
+    b->out[pair] = out ? *out : ds_outputs{};
+    b->args_dirty = true;
+    return DS_OK;
+}
+
+DS_API int ds_batch_run(ds_batch* b, void* stream) {
+    if (!b) return DS_INVALID_ARGUMENT;
+    for (size_t i = 0; i < b->h.size(); ++i) {
+        if (!b->in_l[i]) return b->fail(DS_INVALID_ARGUMENT, "pair " + std::to_string(i) + " has no bound input");
+        if (b->desc[i].raw && !b->calib[b->desc[i].calib].map[0])
+            return b->fail(DS_INVALID_ARGUMENT, "pair " + std::to_string(i) + ": set_rectification() not called");
+    }
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+    return batch_guarded(b, [&]() -> int {
+        if (b->args_dirty) batch_fill_args(b);
+        if (!b->exec) {
+            // Capture once on the batch's own stream; the graph reads the per-pair argument arrays, so
+            // later bindings change what it processes without a new capture.
+            DS_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                batch_enqueue(b, b->stream, true);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(b->stream, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            DS_CUDA(cudaStreamEndCapture(b->stream, &b->graph));
+            DS_CUDA(cudaGraphInstantiate(&b->exec, b->graph, 0));
+        }
+        DS_CUDA(cudaGraphLaunch(b->exec, st));
+        return DS_OK;
+    });
+}
+
+DS_API int ds_batch_run_eager(ds_batch* b, void* stream) {
+    if (!b) return DS_INVALID_ARGUMENT;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : b->stream;
+    return batch_guarded(b, [&]() -> int {
+        if (b->args_dirty) batch_fill_args(b);
+        batch_enqueue(b, st, false);
+        return DS_OK;
+    });
+}
+
+DS_API size_t ds_batch_device_bytes(const ds_batch* b) { return b ? b->bytes : 0; }
+
+DS_API int ds_batch_profile(ds_batch* b, int on) {
+    if (!b) return DS_INVALID_ARGUMENT;
+    return batch_guarded(b, [&]() -> int {
+        if ((on != 0) == b->profile) return DS_OK;
+        if (on && !b->ev[0])
+            for (auto& e : b->ev) DS_CUDA(cudaEventCreate(&e));
+        b->profile = on != 0;
+        if (b->exec) {  // the stage events are part of the captured graph: capture again
+            DS_CUDA(cudaStreamSynchronize(b->stream));
+            cudaGraphExecDestroy(b->exec);
+            cudaGraphDestroy(b->graph);
+            b->exec = nullptr;
+            b->graph = nullptr;
+        }
+        return DS_OK;
+    });
+}
+
+DS_API int ds_batch_stage_ms(ds_batch* b, double* ms) {
+    if (!b || !ms) return DS_INVALID_ARGUMENT;
+    if (!b->profile) return b->fail(DS_INVALID_ARGUMENT, "ds_batch_profile() not enabled");
+    return batch_guarded(b, [&]() -> int {
+        DS_CUDA(cudaEventSynchronize(b->ev[DS_BATCH_STAGES]));
+        for (int i = 0; i < DS_BATCH_STAGES; ++i) {
+            float t = 0.0f;
+            DS_CUDA(cudaEventElapsedTime(&t, b->ev[i], b->ev[i + 1]));
+            ms[i] = t;
+        }
+        return DS_OK;
+    });
+}
+
+DS_API int ds_batch_launches_per_run(const ds_batch* b) {
+    if (!b) return 0;
+    int n = 0;
+    for (const auto& m : b->micro) n += m.launches();
+    return n;
 }
 
 }  // extern "C"

@@ -43,12 +43,27 @@ cudaError_t launch_costs(const KernelCfg& cfg, bool c64, const dsk::CostArgs& a,
 cudaError_t launch_vert(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, cudaStream_t st);
 cudaError_t launch_horz(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, size_t smem, cudaStream_t st);
 
+struct BatchGroupDev;
+
+// Persistent batch launches (one launch walks the blocks of every pair of a kernel-variant group).
+cudaError_t launch_paths_batch(const KernelCfg& cfg, bool c64, bool wide, const dsk::PathArgs* args, const BatchGroupDev& g,
+                               cudaStream_t st);
+cudaError_t launch_wta_batch(const KernelCfg& cfg, bool wide, int ndirs, const dsk::WtaArgs* args, const BatchGroupDev& g,
+                             size_t smem, cudaStream_t st);
+cudaError_t launch_costs_batch(const KernelCfg& cfg, bool c64, const dsk::CostArgs* args, const BatchGroupDev& g,
+                               cudaStream_t st);
+
 #define DS_DECLARE_R(R)                                                                                              \
     cudaError_t launch_paths_r##R(const KernelCfg&, bool, bool, const dsk::PathArgs&, int, int, cudaStream_t);      \
     cudaError_t launch_wta_r##R(const KernelCfg&, bool, const dsk::WtaArgs&, int, size_t, cudaStream_t);              \
     cudaError_t launch_costs_r##R(const KernelCfg&, bool, const dsk::CostArgs&, cudaStream_t);                      \
     cudaError_t launch_vert_r##R(const KernelCfg&, bool, bool, const dsk::FusedArgs&, cudaStream_t);                \
-    cudaError_t launch_horz_r##R(const KernelCfg&, bool, bool, const dsk::FusedArgs&, size_t, cudaStream_t);
+    cudaError_t launch_horz_r##R(const KernelCfg&, bool, bool, const dsk::FusedArgs&, size_t, cudaStream_t);        \
+    cudaError_t launch_paths_batch_r##R(const KernelCfg&, bool, bool, const dsk::PathArgs*, const BatchGroupDev&,    \
+                                        cudaStream_t);                                                               \
+    cudaError_t launch_wta_batch_r##R(const KernelCfg&, bool, int, const dsk::WtaArgs*, const BatchGroupDev&, size_t,\
+                                      cudaStream_t);                                                                 \
+    cudaError_t launch_costs_batch_r##R(const KernelCfg&, bool, const dsk::CostArgs*, const BatchGroupDev&, cudaStream_t);
 DS_DECLARE_R(1)
 DS_DECLARE_R(2)
 DS_DECLARE_R(3)

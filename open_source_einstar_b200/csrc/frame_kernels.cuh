@@ -37,10 +37,10 @@ __device__ __forceinline__ uint32_t remap_sample(const uint8_t* __restrict__ src
     return static_cast<uint32_t>(__float2uint_rz(v));
 }
 
-__global__ void k_rectify(RectifyArgs a) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int side = blockIdx.z;
+__device__ __forceinline__ void rectify_body(const RectifyArgs& a, int bx, int by, int bz) {
+    const int x = bx * blockDim.x + threadIdx.x;
+    const int y = by * blockDim.y + threadIdx.y;
+    const int side = bz;
     if (x >= a.out_w || y >= a.out_h) return;
     const uint8_t* src = a.raw[side];
     const float* mx = a.map_x[side];
@@ -61,21 +61,23 @@ __global__ void k_rectify(RectifyArgs a) {
     a.out[side][static_cast<size_t>(y) * a.out_w + x] = static_cast<uint8_t>(v);
 }
 
+__global__ void k_rectify(RectifyArgs a) { rectify_body(a, blockIdx.x, blockIdx.y, blockIdx.z); }
+
 // ------------------------------------------------------------------------------------------------
 // Census (stereo.cpp:328-346): bit per window neighbour, row-major, centre skipped, MSB first,
 // set when neighbour < centre; 0 within (rx, ry) of the border.
 
 struct CensusArgs {
     const uint8_t* img[2];
-    void* out[2];
-    int w, h, rx, ry;
+    void* out[2];  // (y, x) at y * pitch + x
+    int w, h, rx, ry, pitch;
 };
 
 template <typename W>
-__global__ void k_census(CensusArgs a) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
-    const int side = blockIdx.z;
+__device__ __forceinline__ void census_body(const CensusArgs& a, int bx, int by, int bz) {
+    const int x = bx * blockDim.x + threadIdx.x;
+    const int y = by * blockDim.y + threadIdx.y;
+    const int side = bz;
     if (x >= a.w || y >= a.h) return;
     const uint8_t* img = a.img[side];
     W word = 0;
@@ -89,7 +91,12 @@ __global__ void k_census(CensusArgs a) {
             }
         }
     }
-    static_cast<W*>(a.out[side])[static_cast<size_t>(y) * a.w + x] = word;
+    static_cast<W*>(a.out[side])[static_cast<size_t>(y) * a.pitch + x] = word;
+}
+
+template <typename W>
+__global__ void k_census(CensusArgs a) {
+    census_body<W>(a, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -107,9 +114,9 @@ struct PostArgs {
     float min_depth, max_depth;
 };
 
-__global__ void k_post(PostArgs a) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+__device__ __forceinline__ void post_body(const PostArgs& a, int bx, int by) {
+    const int x = bx * blockDim.x + threadIdx.x;
+    const int y = by * blockDim.y + threadIdx.y;
     if (x >= a.w || y >= a.h) return;
     const size_t i = static_cast<size_t>(y) * a.w + x;
     float d = __ldg(a.disp + i);
@@ -156,6 +163,8 @@ __global__ void k_post(PostArgs a) {
         a.out_depth[i] = z;
     }
 }
+
+__global__ void k_post(PostArgs a) { post_body(a, blockIdx.x, blockIdx.y); }
 
 // Debug: summed path values as u16 [y][x][nd] (the reference's `sum` volume).
 struct SumArgs {

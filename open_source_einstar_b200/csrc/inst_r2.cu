@@ -2,3 +2,4 @@
 #include "launchers.cuh"
 
 DS_DEFINE_R(2)
+DS_DEFINE_BATCH_R(2)

@@ -2,3 +2,4 @@
 #include "launchers.cuh"
 
 DS_DEFINE_R(8)
+DS_DEFINE_BATCH_R(8)

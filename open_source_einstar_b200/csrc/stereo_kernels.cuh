@@ -43,21 +43,21 @@ __device__ __forceinline__ int popcount_word<uint64_t>(uint64_t v) { return __po
 // census instead): u8 [y][x][dp] in the same per-lane chunks as the path values.
 
 struct CostArgs {
-    const void* census_l;
+    const void* census_l;  // (y, x) at y * cpitch + x
     const void* census_r;
     uint8_t* costs;
-    int w, h, nd, dp, min_disp, invalid_cost;
+    int w, h, nd, dp, min_disp, invalid_cost, cpitch;
 };
 
 template <int R, int SEG, typename CW>
-__global__ void __launch_bounds__(256) k_costs(CostArgs a) {
+__device__ __forceinline__ void costs_body(const CostArgs& a, int bx) {
     constexpr int NV = 2 * R;
     const int lane = threadIdx.x & 31, seg = lane / SEG, sl = lane % SEG;
-    const long px = (static_cast<long>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 / SEG) + seg;
+    const long px = (static_cast<long>(bx) * (blockDim.x >> 5) + (threadIdx.x >> 5)) * (32 / SEG) + seg;
     if (px >= static_cast<long>(a.w) * a.h) return;
     const int y = static_cast<int>(px / a.w), x = static_cast<int>(px % a.w);
-    const CW* cl = static_cast<const CW*>(a.census_l) + static_cast<size_t>(y) * a.w;
-    const CW* cr = static_cast<const CW*>(a.census_r) + static_cast<size_t>(y) * a.w;
+    const CW* cl = static_cast<const CW*>(a.census_l) + static_cast<size_t>(y) * a.cpitch;
+    const CW* cr = static_cast<const CW*>(a.census_r) + static_cast<size_t>(y) * a.cpitch;
     const CW vl = __ldg(cl + x);
     const int k0 = sl * NV;
     uint32_t c[R];
@@ -71,6 +71,11 @@ __global__ void __launch_bounds__(256) k_costs(CostArgs a) {
     uint32_t w[chunk_words<NV>()];
     pack<uint8_t, NV>(c, w);
     st_chunk<NV, false>(a.costs + static_cast<size_t>(px) * a.dp + k0, w);
+}
+
+template <int R, int SEG, typename CW>
+__global__ void __launch_bounds__(256) k_costs(CostArgs a) {
+    costs_body<R, SEG, CW>(a, blockIdx.x);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -89,8 +94,9 @@ __global__ void __launch_bounds__(256) k_costs(CostArgs a) {
 // The directions of a frame run concurrently into separate slabs, summed by the WTA kernel.
 
 struct PathArgs {
-    const void* census_l;
+    const void* census_l;  // (y, x) at y * cpitch + x
     const void* census_r;
+    int cpitch;
     const uint8_t* guide;
     const uint8_t* costs;  // materialised costs or nullptr
     void* values;          // [dir][y][x][dp]
@@ -142,16 +148,16 @@ __device__ __forceinline__ uint32_t seg_min(uint32_t v, int seg) {
 
 // PF: depth of the register prefetch ring (the inputs of step s + PF are loaded while step s runs).
 template <int R, int SEG, typename CW, typename ST, bool MAT, int PF>
-__global__ void __launch_bounds__(256) k_paths(PathArgs a) {
+__device__ __forceinline__ void paths_body(const PathArgs& a, int bx, int by) {
     constexpr int NV = 2 * R;
     constexpr int LPW = 32 / SEG;  // lines per warp
     constexpr int CWN = chunk_words<NV>();
     constexpr int VB = NV * static_cast<int>(sizeof(ST));
     const int lane = threadIdx.x & 31, seg = lane / SEG, sl = lane % SEG;
-    const int di = a.dir_base + blockIdx.y;
+    const int di = a.dir_base + by;
     const int dx = c_dir_dx[di], dy = c_dir_dy[di];
     const int nlines = lines_of(dx, dy, a.w, a.h);
-    const int first = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * LPW;
+    const int first = (bx * (blockDim.x >> 5) + (threadIdx.x >> 5)) * LPW;
     if (first >= nlines) return;  // warp-uniform
     const int line = first + seg;
     const bool live = line < nlines;
@@ -188,11 +194,12 @@ __global__ void __launch_bounds__(256) k_paths(PathArgs a) {
         if constexpr (MAT) {
             ld_chunk<NV, LD_NC>(a.costs + (row + cx) * a.dp + k0, pcw[u]);
         } else {
-            pvl[u] = __ldg(cl + row + cx);
+            const size_t crow = static_cast<size_t>(cy) * a.cpitch;
+            pvl[u] = __ldg(cl + crow + cx);
 #pragma unroll
             for (int j = 0; j < NV; ++j) {
                 const int xr = cx - a.min_disp - (k0 + j);
-                pvr[u][j] = (xr >= 0 && xr < a.w) ? __ldg(cr + row + xr) : CW(0);
+                pvr[u][j] = (xr >= 0 && xr < a.w) ? __ldg(cr + crow + xr) : CW(0);
             }
         }
     };
@@ -274,6 +281,11 @@ __global__ void __launch_bounds__(256) k_paths(PathArgs a) {
     }
 }
 
+template <int R, int SEG, typename CW, typename ST, bool MAT, int PF>
+__global__ void __launch_bounds__(256) k_paths(PathArgs a) {
+    paths_body<R, SEG, CW, ST, MAT, PF>(a, blockIdx.x, blockIdx.y);
+}
+
 // ------------------------------------------------------------------------------------------------
 // Winner-takes-all left + right and the L-R check (stereo.cpp:411-461), one CTA per row.
 // A segment of SEG lanes takes one pixel: the direction slabs are summed as 16-bit lanes (the
@@ -310,14 +322,14 @@ __device__ __forceinline__ uint32_t pick16(const uint32_t (&v)[R], int j) {  // 
 }
 
 template <int R, int SEG, typename ST, int NDIRS>
-__global__ void __launch_bounds__(256) k_wta(WtaArgs a) {
+__device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
     constexpr int NV = 2 * R;
     constexpr int VB = NV * static_cast<int>(sizeof(ST));
     constexpr int VW = chunk_words<VB>();
     extern __shared__ uint32_t smem[];
     uint32_t* rkey = smem;                                // [w]
     float* dleft = reinterpret_cast<float*>(smem + a.w);  // [w]
-    const int y = blockIdx.x;
+    const int y = bx;
     const int lane = threadIdx.x & 31, seg = lane / SEG, sl = lane % SEG;
     const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int i = threadIdx.x; i < a.w; i += blockDim.x) rkey[i] = 0xFFFFFFFFu;
@@ -417,6 +429,11 @@ __global__ void __launch_bounds__(256) k_wta(WtaArgs a) {
         }
         a.disp[static_cast<size_t>(y) * a.w + x] = d;
     }
+}
+
+template <int R, int SEG, typename ST, int NDIRS>
+__global__ void __launch_bounds__(256) k_wta(WtaArgs a) {
+    wta_body<R, SEG, ST, NDIRS>(a, blockIdx.x);
 }
 
 }  // namespace dsk

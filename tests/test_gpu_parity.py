@@ -233,3 +233,78 @@ def test_odd_and_degenerate_sizes(cuda, port, w, h, nd, mind):
             s.set_kernel_config(cfg["regs_per_lane"], cfg["lanes_per_line"], False, 1, 64, 4, fused, 1)
             got = s.compute(left, right).disparity
         assert same_bits(got, want), f"{w}x{h} fused={fused}: {mismatch_report(got, want)}"
+
+
+def test_batch_matches_per_pair_runs(cuda, port):
+    """Uneven sizes and disparity ranges, rectified and raw pairs (two calibrations), kernel variants:
+    one batched graph launch equals per-pair runs bit for bit, also after replay and re-binding."""
+    import torch
+    from open_source_einstar_b200 import (CudaStereo, PairDesc, RectifiedGeometry, RemapTable, SgmParams, StereoBatch,
+                                          StereoParams, synth)
+    specs = [(320, 256, 64, None), (160, 128, 96, None), (240, 192, 128, None), (200, 136, 192, None),
+             (160, 128, 40, {"regs_per_lane": 3, "lanes_per_line": 16, "materialize_costs": 0}),
+             (128, 96, 64, {"regs_per_lane": 1, "lanes_per_line": 32, "materialize_costs": 1, "prefetch_steps": 8})]
+    rect_pairs = [synth.plane_sphere_pair(seed=40 + i, width=w, height=h, f=w * 1.4, num_disparities=d)
+                  for i, (w, h, d, _) in enumerate(specs)]
+    raw_specs = [(256, 192, 0), (256, 192, 0), (192, 160, 1)]
+    raw_pairs = [synth.raw_objects_pair(seed=60 + i, width=w, height=h, f=w * 0.86, num_disparities=64, n_objects=6,
+                                        device="cuda") for i, (w, h, _) in enumerate(raw_specs)]
+    descs, inputs, want = [], [], []
+    for (w, h, d, k), pr in zip(specs, rect_pairs):
+        sp = StereoParams(sgm=SgmParams(min_disparity=pr.min_disparity, num_disparities=d))
+        descs.append(PairDesc(w, h, sp, geometry=RectifiedGeometry(pr.f, 0, 0, pr.baseline), kernel=k))
+        inputs.append((pr.left, pr.right))
+    calibs = {}
+    for (w, h, ci), pr in zip(raw_specs, raw_pairs):
+        sp = StereoParams(sgm=SgmParams(min_disparity=pr.min_disparity, num_disparities=64))
+        descs.append(PairDesc(w, h, sp, raw=True, calib=ci))
+        inputs.append((pr.left, pr.right))
+        calibs.setdefault(ci, (pr.maps, w, h))
+    for d, (l, r), i in zip(descs, inputs, range(len(descs))):
+        with CudaStereo.create(d.params, d.width, d.height) as s:
+            if d.kernel:
+                kk = {"path_warps_per_block": 4, "wta_threads": 256, "prefetch_steps": 4, **d.kernel}
+                s.set_kernel_config(kk["regs_per_lane"], kk["lanes_per_line"], bool(kk.get("materialize_costs", 0)),
+                                    kk["path_warps_per_block"], kk["wta_threads"], kk["prefetch_steps"])
+            if d.raw:
+                (mlx, mly), (mrx, mry) = calibs[d.calib][0]
+                s.set_rectification(RemapTable(mlx, mly), RemapTable(mrx, mry), d.width, d.height)
+                res = s.compute_raw(l, r)
+            else:
+                if d.geometry is not None:
+                    s.set_point_params(d.geometry, d.min_depth, d.max_depth)
+                res = s.compute(l, r)
+        want.append(res)
+    b = StereoBatch(descs, n_calib=2)
+    for ci, ((mlx, mly), (mrx, mry)), w, h in [(ci, v[0], v[1], v[2]) for ci, v in calibs.items()]:
+        b.set_rectification(ci, RemapTable(mlx, mly), RemapTable(mrx, mry), w, h)
+    dev_in, dev_out = [], []
+    for i, (l, r) in enumerate(inputs):
+        dl, dr = torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()
+        o = {"disparity": torch.empty(l.shape, dtype=torch.float32, device="cuda"),
+             "disparity_u16": torch.empty(l.shape, dtype=torch.int16, device="cuda")}
+        if descs[i].geometry is not None:
+            o["depth"] = torch.empty(l.shape, dtype=torch.float32, device="cuda")
+        b.bind(i, dl, dr, o)
+        dev_in.append((dl, dr))
+        dev_out.append(o)
+    st = torch.cuda.current_stream()
+    for rep in range(2):
+        for o in dev_out:
+            o["disparity"].fill_(7.0)
+        b.run(stream=st)
+        st.synchronize()
+        for i, (o, wres) in enumerate(zip(dev_out, want)):
+            got = o["disparity"].cpu().numpy()
+            assert same_bits(got, wres.disparity), f"pair {i} rep {rep}: {mismatch_report(got, wres.disparity)}"
+            assert np.array_equal(o["disparity_u16"].cpu().numpy().view(np.uint16), wres.disparity_u16)
+            if "depth" in o:
+                assert same_bits(o["depth"].cpu().numpy(), wres.depth)
+    # re-bind: pair 6 takes pair 7's inputs (same size and calibration); the captured graph is replayed
+    b.bind(6, dev_in[7][0], dev_in[7][1], dev_out[6])
+    b.run(stream=st)
+    st.synchronize()
+    assert same_bits(dev_out[6]["disparity"].cpu().numpy(), want[7].disparity)
+    # persistent launches: one per stage and kernel variant, far fewer than the per-pair launches
+    assert b.launches_per_run < 5 * len(descs)
+    b.close()
