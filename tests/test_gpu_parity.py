@@ -275,36 +275,37 @@ def test_batch_matches_per_pair_runs(cuda, port):
                     s.set_point_params(d.geometry, d.min_depth, d.max_depth)
                 res = s.compute(l, r)
         want.append(res)
-    b = StereoBatch(descs, n_calib=2)
-    for ci, ((mlx, mly), (mrx, mry)), w, h in [(ci, v[0], v[1], v[2]) for ci, v in calibs.items()]:
-        b.set_rectification(ci, RemapTable(mlx, mly), RemapTable(mrx, mry), w, h)
-    dev_in, dev_out = [], []
-    for i, (l, r) in enumerate(inputs):
-        dl, dr = torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()
-        o = {"disparity": torch.empty(l.shape, dtype=torch.float32, device="cuda"),
-             "disparity_u16": torch.empty(l.shape, dtype=torch.int16, device="cuda")}
-        if descs[i].geometry is not None:
-            o["depth"] = torch.empty(l.shape, dtype=torch.float32, device="cuda")
-        b.bind(i, dl, dr, o)
-        dev_in.append((dl, dr))
-        dev_out.append(o)
-    st = torch.cuda.current_stream()
-    for rep in range(2):
-        for o in dev_out:
-            o["disparity"].fill_(7.0)
+    for micro_batch, branches in ((len(descs), 1), (0, 0)):  # all pairs per launch; the default schedule
+        b = StereoBatch(descs, n_calib=2, micro_batch=micro_batch, branches=branches)
+        for ci, ((mlx, mly), (mrx, mry)), w, h in [(ci, v[0], v[1], v[2]) for ci, v in calibs.items()]:
+            b.set_rectification(ci, RemapTable(mlx, mly), RemapTable(mrx, mry), w, h)
+        dev_in, dev_out = [], []
+        for i, (l, r) in enumerate(inputs):
+            dl, dr = torch.from_numpy(l).cuda(), torch.from_numpy(r).cuda()
+            o = {"disparity": torch.empty(l.shape, dtype=torch.float32, device="cuda"),
+                 "disparity_u16": torch.empty(l.shape, dtype=torch.int16, device="cuda")}
+            if descs[i].geometry is not None:
+                o["depth"] = torch.empty(l.shape, dtype=torch.float32, device="cuda")
+            b.bind(i, dl, dr, o)
+            dev_in.append((dl, dr))
+            dev_out.append(o)
+        st = torch.cuda.current_stream()
+        for rep in range(2):
+            for o in dev_out:
+                o["disparity"].fill_(7.0)
+            b.run(stream=st)
+            st.synchronize()
+            for i, (o, wres) in enumerate(zip(dev_out, want)):
+                got = o["disparity"].cpu().numpy()
+                assert same_bits(got, wres.disparity), f"pair {i} rep {rep}: {mismatch_report(got, wres.disparity)}"
+                assert np.array_equal(o["disparity_u16"].cpu().numpy().view(np.uint16), wres.disparity_u16)
+                if "depth" in o:
+                    assert same_bits(o["depth"].cpu().numpy(), wres.depth)
+        # re-bind: pair 6 takes pair 7's inputs (same size and calibration); the captured graph is replayed
+        b.bind(6, dev_in[7][0], dev_in[7][1], dev_out[6])
         b.run(stream=st)
         st.synchronize()
-        for i, (o, wres) in enumerate(zip(dev_out, want)):
-            got = o["disparity"].cpu().numpy()
-            assert same_bits(got, wres.disparity), f"pair {i} rep {rep}: {mismatch_report(got, wres.disparity)}"
-            assert np.array_equal(o["disparity_u16"].cpu().numpy().view(np.uint16), wres.disparity_u16)
-            if "depth" in o:
-                assert same_bits(o["depth"].cpu().numpy(), wres.depth)
-    # re-bind: pair 6 takes pair 7's inputs (same size and calibration); the captured graph is replayed
-    b.bind(6, dev_in[7][0], dev_in[7][1], dev_out[6])
-    b.run(stream=st)
-    st.synchronize()
-    assert same_bits(dev_out[6]["disparity"].cpu().numpy(), want[7].disparity)
-    # persistent launches: one per stage and kernel variant, far fewer than the per-pair launches
-    assert b.launches_per_run < 5 * len(descs)
-    b.close()
+        assert same_bits(dev_out[6]["disparity"].cpu().numpy(), want[7].disparity)
+        if branches == 1:  # one persistent launch per stage and kernel variant for all pairs
+            assert b.launches_per_run < 5 * len(descs) // 2
+        b.close()
