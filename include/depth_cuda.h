@@ -239,6 +239,24 @@ DS_API int ds_batch_launches_per_run(const ds_batch* batch);
 DS_API int ds_batch_profile(ds_batch* batch, int on);
 DS_API int ds_batch_stage_ms(ds_batch* batch, double* ms);
 
+/* ---- Disparity without device allocation (no counterpart in the reference) -----------------------
+ * For callers that cannot allocate device memory when they need a disparity map: processes with a fixed
+ * device-memory budget that forbid allocations after start-up, real-time loops where an allocation may
+ * block or fail, frameworks whose own allocator owns the device. Computes what ds_compute_device computes
+ * before its median (census, path aggregation, WTA, left/right check; the reference's sgm_disparity,
+ * libs/depth/src/stereo.cpp:361-463) from `left`/`right` (device, tightly packed width x height u8) into
+ * `disparity` (device, width x height f32), enqueued on `stream` (a cudaStream_t; NULL = the default
+ * stream). Allocates nothing: all intermediates live in one static 16 MiB device array that every GPU
+ * loading the library keeps until the process exits. A request whose intermediates exceed it
+ * (two W x H census images of 4- or 8-byte words, plus P paths x W x H x disparities of 1- or 2-byte path
+ * values; about 320 x 240 at 32 disparities and 4 paths fits) is rejected with DS_INVALID_ARGUMENT and a
+ * message giving the bytes needed. The first call on each device looks up the array's device address
+ * (with that device current) and should come before any stream capture. Calls share the array: calls
+ * whose work overlaps on the GPU (other streams, other threads) race and must be serialised by the
+ * caller. Errors: ds_last_global_error(). */
+DS_API int ds_sgm_disparity_noalloc(const uint8_t* left, const uint8_t* right, int width, int height,
+                                    const ds_sgm_params* sgm, int subpixel, float* disparity, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

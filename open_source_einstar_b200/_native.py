@@ -92,6 +92,7 @@ SIGNATURES = {
     "ds_batch_launches_per_run": (_i, [_vp]),
     "ds_batch_profile": (_i, [_vp, _i]),
     "ds_batch_stage_ms": (_i, [_vp, _vp]),
+    "ds_sgm_disparity_noalloc": (_i, [_vp, _vp, _i, _i, C.POINTER(SgmParamsC), _i, _vp, _vp]),
 }
 
 _lib = None

@@ -488,6 +488,9 @@ int guarded(ds_handle* h, F&& f) {
 
 namespace ds {
 
+void set_global_error(const char* message) { g_error = message ? message : ""; }
+void count_launches(int n) { g_launches += static_cast<uint64_t>(n); }
+
 bool cfg_supported(int R, int seg) {
     if (seg == 16) return R == 1 || R == 2 || R == 3 || R == 4;
     if (seg == 32) return R == 1 || R == 2 || R == 3 || R == 4 || R == 6 || R == 8;

@@ -34,6 +34,10 @@ struct KernelCfg {
 // Configurations that have kernels: SEG 16 with R in {1,2,3,4}; SEG 32 with R in {1,2,3,4,6,8}.
 bool cfg_supported(int R, int seg);
 
+// Library-internal bookkeeping shared by the translation units that launch kernels.
+void set_global_error(const char* message);  // the text ds_last_global_error() returns
+void count_launches(int n);                    // kernels launched (ds_kernel_launches)
+
 // Returns a CUDA error (cudaSuccess on success). `c64`: 64-bit census words; `wide`: u16 path values.
 cudaError_t launch_paths(const KernelCfg& cfg, bool c64, bool wide, const dsk::PathArgs& a, int ndirs, int max_lines,
                          cudaStream_t st);

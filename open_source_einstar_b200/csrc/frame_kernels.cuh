@@ -1,5 +1,5 @@
 // Per-frame kernels around the SGM core (sm_100a): rectification remap, census, median + outputs.
-// Included by one translation unit only (depth_cuda.cu).
+// The non-template kernels have internal linkage, so that several translation units may include this.
 #pragma once
 
 #include "stereo_kernels.cuh"
@@ -61,7 +61,7 @@ __device__ __forceinline__ void rectify_body(const RectifyArgs& a, int bx, int b
     a.out[side][static_cast<size_t>(y) * a.out_w + x] = static_cast<uint8_t>(v);
 }
 
-__global__ void k_rectify(RectifyArgs a) { rectify_body(a, blockIdx.x, blockIdx.y, blockIdx.z); }
+static __global__ void k_rectify(RectifyArgs a) { rectify_body(a, blockIdx.x, blockIdx.y, blockIdx.z); }
 
 // ------------------------------------------------------------------------------------------------
 // Census (stereo.cpp:328-346): bit per window neighbour, row-major, centre skipped, MSB first,
@@ -164,7 +164,7 @@ __device__ __forceinline__ void post_body(const PostArgs& a, int bx, int by) {
     }
 }
 
-__global__ void k_post(PostArgs a) { post_body(a, blockIdx.x, blockIdx.y); }
+static __global__ void k_post(PostArgs a) { post_body(a, blockIdx.x, blockIdx.y); }
 
 // Debug: summed path values as u16 [y][x][nd] (the reference's `sum` volume).
 struct SumArgs {
@@ -175,7 +175,7 @@ struct SumArgs {
 };
 
 template <typename ST>
-__global__ void k_debug_sums(SumArgs a) {
+static __global__ void k_debug_sums(SumArgs a) {
     const size_t n = static_cast<size_t>(a.w) * a.h * a.nd;
     const ST* v = static_cast<const ST*>(a.values);
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
