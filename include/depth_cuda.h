@@ -156,8 +156,10 @@ DS_API size_t ds_device_bytes(const ds_handle* handle);
 /* Per-stage device times, the counterpart of the reference's per-stage GPU profile
  * (libs/gpu/include/einstar/gpu/profile.hpp:14-32; stage labels metal_stereo.cpp:480-652). When enabled,
  * every frame records CUDA events between its stages on the stream it runs on; nothing is serialised.
- * Stages: 0 rectify, 1 census, 2 SGM paths, 3 WTA + L-R check, 4 median + outputs (DS_STAGES). */
-#define DS_STAGES 5
+ * Stages: 0 rectify, 1 census, 2 costs (0 when the path kernels recompute them), 3 SGM paths,
+ * 4 WTA + L-R check, 5 median + outputs (DS_STAGES). Up to 4096 frames may be pending between two
+ * ds_profile_collect calls; a frame beyond that fails with DS_IO. */
+#define DS_STAGES 6
 DS_API int ds_profile_enable(ds_handle* handle, int on);
 /* Waits for the profiled frames since the last call and writes up to `max_frames` rows of DS_STAGES
  * milliseconds each to `stage_ms` (row = frame, oldest first); `*frames` = rows written. */
@@ -205,7 +207,10 @@ typedef struct ds_batch ds_batch;
 
 /* Scheduling of a batch: pairs (heaviest first) are cut into micro-batches of `micro_batch` pairs that go
  * through all stages back to back (so a pair's volumes are consumed while still in L2), and the
- * micro-batches run round-robin on `branches` parallel branches of the graph. 0 = defaults (1, 4). */
+ * micro-batches run round-robin on `branches` parallel branches of the graph. 0 = defaults (1, 4).
+ * Micro-batches on one branch run one after another, so they share cost and path-value volumes: the
+ * batch holds branches x micro_batch volumes (each sized for the largest pair it serves), not one per
+ * pair. */
 typedef struct ds_batch_options {
     int micro_batch;
     int branches;
@@ -231,6 +236,8 @@ DS_API int ds_batch_run_eager(ds_batch* batch, void* stream);
 DS_API size_t ds_batch_device_bytes(const ds_batch* batch);
 /* Kernel launches per run (persistent launches: one per stage and kernel variant). */
 DS_API int ds_batch_launches_per_run(const ds_batch* batch);
+/* The schedule in effect (defaults resolved). */
+DS_API int ds_batch_get_options(const ds_batch* batch, ds_batch_options* out);
 /* Stage timing of the last run, measured on the first micro-batch (CUDA events captured into the graph
  * between its stages, while the other branches run beside it):
  * 0 rectify, 1 census, 2 costs, 3 SGM paths, 4 WTA + L-R, 5 median + outputs (DS_BATCH_STAGES).
@@ -238,6 +245,74 @@ DS_API int ds_batch_launches_per_run(const ds_batch* batch);
 #define DS_BATCH_STAGES 6
 DS_API int ds_batch_profile(ds_batch* batch, int on);
 DS_API int ds_batch_stage_ms(ds_batch* batch, double* ms);
+
+/* ---- Request server: continuous batching of frames as they arrive (no counterpart in the reference,
+ * whose frontend runs one camera pair synchronously, libs/pipeline/src/stereo_frontend.cpp:302-330) ------
+ * A worker thread admits submitted frames in arrival order as soon as a slot (a CUDA stream with its own
+ * frame buffers) is free and the cost / path-value volumes stay within `volume_budget_bytes`; admitted
+ * frames run concurrently on their slots' streams. Volume memory is owned by the slots and reused: the
+ * sum of all slots' volume buffers never exceeds the budget. Calibrations (remap tables, geometry) stay
+ * resident on the device. Inputs are copied from and results to the caller's host buffers, which must
+ * stay valid until the frame's completion has been polled; pinned host memory lets the copies overlap
+ * other frames' work. */
+typedef struct ds_server ds_server;
+
+typedef struct ds_server_options {
+    size_t volume_budget_bytes; /* 0: 40 GB */
+    int max_slots;              /* frames on the GPU at once; 0: 8 */
+    int max_pending;            /* queued frames before ds_server_submit returns DS_BUSY; 0: 4096 */
+} ds_server_options;
+
+typedef struct ds_request {
+    int calib;                /* resident calibration of a raw pair; -1: the pair is already rectified */
+    int width, height;        /* stereo (rectified) size */
+    ds_stereo_params params;
+    const uint8_t* left;      /* host; raw_width x raw_height (calib >= 0) or width x height */
+    const uint8_t* right;
+    ptrdiff_t stride;         /* bytes between rows of left and right */
+    ds_outputs out;           /* host buffers, width x height (rect_left / rect_right unused) */
+    uint64_t tag;             /* returned with the completion */
+} ds_request;
+
+typedef struct ds_completion {
+    uint64_t ticket;
+    uint64_t tag;
+    int status;               /* DS_OK, or the failure's code (text: ds_server_last_error) */
+    double queue_ms;          /* submit -> admission to a slot */
+    double gpu_ms;            /* device time of the frame on its slot, copies included */
+    double latency_ms;        /* submit -> results in host memory */
+} ds_completion;
+
+typedef struct ds_server_stats {
+    uint64_t submitted, completed, failed;
+    int pending, running, peak_running, slots;
+    size_t running_volume_bytes, peak_running_volume_bytes;
+    size_t volume_bytes;      /* volume memory held by the slots (<= the budget) */
+    size_t device_bytes;      /* all device memory of the server */
+} ds_server_stats;
+
+/* Creates the server and its worker thread on the current device. */
+DS_API int ds_server_create(const ds_server_options* options, ds_server** out);
+/* Finishes the frames on the GPU, drops the pending ones and frees everything. */
+DS_API void ds_server_destroy(ds_server* server);
+DS_API const char* ds_server_last_error(const ds_server* server);
+/* Resident calibration `calib` (>= 0): remap tables as ds_set_rectification, and the geometry used for
+ * depth (NULL: frames of this calibration produce no depth). Replacing a calibration waits for the
+ * frames in flight. */
+DS_API int ds_server_add_calibration(ds_server* server, int calib, const float* map_left_x, const float* map_left_y,
+                                     const float* map_right_x, const float* map_right_y, int map_width, int map_height,
+                                     int raw_width, int raw_height, const ds_geometry* geometry, float min_depth_mm,
+                                     float max_depth_mm);
+/* Allocates, ahead of time, the buffers of `count` slots for frames of this size, parameters and
+ * calibration (-1: rectified), so that serving them allocates nothing. */
+DS_API int ds_server_reserve(ds_server* server, int width, int height, const ds_stereo_params* params, int calib,
+                             int count);
+/* Queues a frame (validated here) and returns at once; *ticket identifies its completion. */
+DS_API int ds_server_submit(ds_server* server, const ds_request* request, uint64_t* ticket);
+/* Waits up to timeout_ms (0: no wait, < 0: no limit) for at least one completion and returns up to `max`
+ * of them, oldest first; *n = the number written. */
+DS_API int ds_server_poll(ds_server* server, ds_completion* out, int max, int* n, int timeout_ms);
+DS_API int ds_server_get_stats(ds_server* server, ds_server_stats* out);
 
 /* ---- Disparity without device allocation (no counterpart in the reference) -----------------------
  * For callers that cannot allocate device memory when they need a disparity map: processes with a fixed

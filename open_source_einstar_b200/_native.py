@@ -59,6 +59,28 @@ class BatchOptionsC(C.Structure):
     _fields_ = [("micro_batch", C.c_int), ("branches", C.c_int)]
 
 
+class ServerOptionsC(C.Structure):
+    _fields_ = [("volume_budget_bytes", C.c_size_t), ("max_slots", C.c_int), ("max_pending", C.c_int)]
+
+
+class RequestC(C.Structure):
+    _fields_ = [("calib", C.c_int), ("width", C.c_int), ("height", C.c_int), ("params", StereoParamsC),
+                ("left", C.c_void_p), ("right", C.c_void_p), ("stride", C.c_ssize_t), ("out", OutputsC),
+                ("tag", C.c_uint64)]
+
+
+class CompletionC(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("tag", C.c_uint64), ("status", C.c_int), ("queue_ms", C.c_double),
+                ("gpu_ms", C.c_double), ("latency_ms", C.c_double)]
+
+
+class ServerStatsC(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("pending", C.c_int), ("running", C.c_int), ("peak_running", C.c_int), ("slots", C.c_int),
+                ("running_volume_bytes", C.c_size_t), ("peak_running_volume_bytes", C.c_size_t),
+                ("volume_bytes", C.c_size_t), ("device_bytes", C.c_size_t)]
+
+
 # Every symbol include/depth_cuda.h declares: name -> (restype, argtypes).
 _vp, _i, _f, _sz = C.c_void_p, C.c_int, C.c_float, C.c_size_t
 SIGNATURES = {
@@ -90,8 +112,17 @@ SIGNATURES = {
     "ds_batch_run_eager": (_i, [_vp, _vp]),
     "ds_batch_device_bytes": (_sz, [_vp]),
     "ds_batch_launches_per_run": (_i, [_vp]),
+    "ds_batch_get_options": (_i, [_vp, C.POINTER(BatchOptionsC)]),
     "ds_batch_profile": (_i, [_vp, _i]),
     "ds_batch_stage_ms": (_i, [_vp, _vp]),
+    "ds_server_create": (_i, [C.POINTER(ServerOptionsC), C.POINTER(_vp)]),
+    "ds_server_destroy": (None, [_vp]),
+    "ds_server_last_error": (C.c_char_p, [_vp]),
+    "ds_server_add_calibration": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _i, _i, _i, _i, C.POINTER(GeometryC), _f, _f]),
+    "ds_server_reserve": (_i, [_vp, _i, _i, C.POINTER(StereoParamsC), _i, _i]),
+    "ds_server_submit": (_i, [_vp, C.POINTER(RequestC), C.POINTER(C.c_uint64)]),
+    "ds_server_poll": (_i, [_vp, C.POINTER(CompletionC), _i, C.POINTER(_i), _i]),
+    "ds_server_get_stats": (_i, [_vp, C.POINTER(ServerStatsC)]),
     "ds_sgm_disparity_noalloc": (_i, [_vp, _vp, _i, _i, C.POINTER(SgmParamsC), _i, _vp, _vp]),
 }
 

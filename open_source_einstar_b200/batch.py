@@ -118,3 +118,18 @@ class StereoBatch:
     @property
     def launches_per_run(self) -> int:
         return int(N.lib().ds_batch_launches_per_run(self._b))
+
+    def _options(self) -> N.BatchOptionsC:
+        o = N.BatchOptionsC()
+        self._check(N.lib().ds_batch_get_options(self._b, C.byref(o)))
+        return o
+
+    @property
+    def micro_batch(self) -> int:
+        """Pairs per micro-batch (all stages of a micro-batch run back to back)."""
+        return int(self._options().micro_batch)
+
+    @property
+    def branches(self) -> int:
+        """Parallel graph branches the micro-batches are spread over."""
+        return int(self._options().branches)

@@ -17,13 +17,14 @@
 #include "dispatch.h"
 #include "frame_kernels.cuh"
 #include "fused_kernels.cuh"
+#include "internal.h"
 
 namespace {
 
 thread_local std::string g_error;
 std::atomic<uint64_t> g_launches{0};
 
-constexpr int kProfileRing = 256;  // frames whose stage events can be pending at once
+constexpr int kProfileRing = 4096;  // frames whose stage events can be pending at once
 
 struct CudaFailure {
     cudaError_t err;
@@ -76,6 +77,7 @@ struct ds_handle {
     float* d_map[4] = {nullptr, nullptr, nullptr, nullptr};  // lx, ly, rx, ry
     int map_w = 0, map_h = 0, raw_w = 0, raw_h = 0;
     bool have_rect = false;
+    bool maps_external = false;  // d_map bound by an owner (the request server's resident calibrations)
     void* d_census[2] = {nullptr, nullptr};    // padded census: (y, x) at y * cpitch + x, inside census_raw
     void* census_raw[2] = {nullptr, nullptr};
     int cpitch = 0, cguard = 0;
@@ -87,6 +89,9 @@ struct ds_handle {
     size_t values_bytes = 0;
     uint8_t* d_costs = nullptr;  // materialised costs (cfg.materialize)
     size_t costs_bytes = 0;
+    // Volumes (d_values, d_costs) owned by a batch that shares them between pairs run one after another;
+    // the handle only sizes them.
+    bool external_volumes = false;
     float* d_disp_lr = nullptr;
     float* d_out_disp = nullptr;
     float* d_out_conf = nullptr;
@@ -128,10 +133,13 @@ void release(ds_handle* h) {
     };
     for (auto* p : h->rect_raw) f(p);
     for (auto* p : h->d_raw) f(p);
-    for (auto* p : h->d_map) f(p);
+    if (!h->maps_external)
+        for (auto* p : h->d_map) f(p);
     for (auto* p : h->census_raw) f(p);
-    f(h->d_values);
-    f(h->d_costs);
+    if (!h->external_volumes) {
+        f(h->d_values);
+        f(h->d_costs);
+    }
     f(h->d_disp_lr);
     f(h->d_out_disp);
     f(h->d_out_conf);
@@ -212,6 +220,17 @@ dsk::FusedArgs fused_args(const ds_handle* h) {
     return a;
 }
 
+// The materialised cost volume (nothing when the path kernels recompute costs from the census).
+void launch_costs(ds_handle* h, cudaStream_t st) {
+    if (h->cfg.fused || !h->cfg.materialize) return;
+    const auto& sg = h->p.sgm;
+    const int window = (2 * sg.census_radius_x + 1) * (2 * sg.census_radius_y + 1);
+    dsk::CostArgs c{h->d_census[0], h->d_census[1], h->d_costs, h->w, h->h, h->nd, h->dp, sg.min_disparity, window,
+                    h->cpitch};
+    DS_CUDA(ds::launch_costs(h->cfg, h->census64, c, st));
+    ++g_launches;
+}
+
 void launch_paths(ds_handle* h, cudaStream_t st) {
     if (h->cfg.fused) {
         DS_CUDA(ds::launch_vert(h->cfg, h->census64, h->s16, fused_args(h), st));
@@ -220,12 +239,6 @@ void launch_paths(ds_handle* h, cudaStream_t st) {
     }
     const auto& sg = h->p.sgm;
     const int window = (2 * sg.census_radius_x + 1) * (2 * sg.census_radius_y + 1);
-    if (h->cfg.materialize) {
-        dsk::CostArgs c{h->d_census[0], h->d_census[1], h->d_costs, h->w, h->h, h->nd, h->dp, sg.min_disparity, window,
-                        h->cpitch};
-        DS_CUDA(ds::launch_costs(h->cfg, h->census64, c, st));
-        ++g_launches;
-    }
     dsk::PathArgs a{};
     a.census_l = h->d_census[0];
     a.census_r = h->d_census[1];
@@ -306,6 +319,15 @@ void size_config_buffers(ds_handle* h) {
     }
     const size_t slab = static_cast<size_t>(h->h + 2 * g) * h->w * h->dp * (h->s16 ? 2 : 1);  // fused, bytes
     const size_t vb = h->cfg.fused ? 2 * slab : h->dir_stride * h->ndirs * (h->wide ? 2 : 1);
+    const size_t cb = h->cfg.materialize && !h->cfg.fused ? n * static_cast<size_t>(h->dp) : 0;
+    if (h->external_volumes) {  // a batch binds shared volumes later (never the fused kernels)
+        h->values_bytes = vb;
+        h->costs_bytes = cb;
+        h->d_values = nullptr;
+        h->d_costs = nullptr;
+        h->d_S = h->d_T = nullptr;
+        return;
+    }
     if (vb != h->values_bytes) {
         if (h->d_values) {
             cudaFree(h->d_values);
@@ -323,7 +345,6 @@ void size_config_buffers(ds_handle* h) {
     } else {
         h->d_S = h->d_T = nullptr;
     }
-    const size_t cb = h->cfg.materialize && !h->cfg.fused ? n * static_cast<size_t>(h->dp) : 0;
     if (cb != h->costs_bytes) {
         if (h->d_costs) {
             cudaFree(h->d_costs);
@@ -345,7 +366,7 @@ struct StageMarks {
     }
 };
 
-// The whole frame on `st`: [rectify] -> census -> paths -> WTA + L-R -> median + outputs.
+// The whole frame on `st`: [rectify] -> census -> [costs] -> paths -> WTA + L-R -> median + outputs.
 void enqueue_frame(ds_handle* h, const uint8_t* left, const uint8_t* right, bool raw, const ds_outputs& out,
                    cudaStream_t st) {
     const uint8_t* img[2] = {left, right};
@@ -400,10 +421,12 @@ void enqueue_frame(ds_handle* h, const uint8_t* left, const uint8_t* right, bool
         ++g_launches;
     }
     marks.mark(2);
-    launch_paths(h, st);
+    launch_costs(h, st);
     marks.mark(3);
-    launch_wta(h, st);
+    launch_paths(h, st);
     marks.mark(4);
+    launch_wta(h, st);
+    marks.mark(5);
     {
         dsk::PostArgs q{};
         q.disp = h->d_disp_lr;
@@ -424,7 +447,7 @@ void enqueue_frame(ds_handle* h, const uint8_t* left, const uint8_t* right, bool
         dsk::k_post<<<g, b, 0, st>>>(q);
         ++g_launches;
     }
-    marks.mark(5);
+    marks.mark(6);
     DS_CUDA(cudaGetLastError());
 }
 
@@ -603,30 +626,9 @@ __global__ void kb_post(const PostArgs* __restrict__ args, const int* __restrict
 
 }  // namespace dsk
 
-extern "C" {
+namespace {
 
-DS_API void ds_default_params(ds_stereo_params* p) {
-    if (!p) return;
-    *p = ds_stereo_params{};
-    p->pyramid_levels = 0;
-    p->sgm.min_disparity = 0;
-    p->sgm.num_disparities = 64;
-    p->sgm.census_radius_x = 2;
-    p->sgm.census_radius_y = 2;
-    p->sgm.p1 = 8;
-    p->sgm.p2 = 96;
-    p->sgm.adaptive_p2 = 1;
-    p->sgm.eight_paths = 0;
-    p->sgm.slant_steps = 1;
-    p->sgm.uniqueness = 0.9f;
-    p->sgm.lr_max_diff = 1;
-    p->subpixel = 1;
-    p->median = 1;
-}
-
-DS_API const char* ds_last_global_error(void) { return g_error.c_str(); }
-
-DS_API int ds_create(const ds_stereo_params* params, int width, int height, ds_handle** out) {
+int create_handle(const ds_stereo_params* params, int width, int height, bool external_volumes, ds_handle** out) {
     if (!params || !out) {
         g_error = "null argument";
         return DS_INVALID_ARGUMENT;
@@ -655,6 +657,7 @@ DS_API int ds_create(const ds_stereo_params* params, int width, int height, ds_h
         h->wide = params->wide_costs || window + params->sgm.p2 > 255;
         h->s16 = h->wide || 2 * (window + params->sgm.p2) > 255;
         h->cfg.fused = false;  // the fused pairs are selectable (ds_set_kernel_config / autotuner)
+        h->external_volumes = external_volumes;
         if (h->ndirs == 4) {
             const int rows_max = static_cast<int>(kMaxSmem / (static_cast<size_t>(width) * 4 * dsk::kHorzWordsPerPixel));
             h->cfg.horz_warps = std::max(1, std::min(4, rows_max / (32 / h->cfg.seg)));
@@ -685,6 +688,94 @@ DS_API int ds_create(const ds_stereo_params* params, int width, int height, ds_h
     return DS_OK;
 }
 
+}  // namespace
+
+namespace ds {
+
+int validate_params(const ds_stereo_params& params, int width, int height, std::string& message) {
+    return validate(params, width, height, message);
+}
+
+int create_shared_volume_handle(const ds_stereo_params* params, int width, int height, ds_handle** out) {
+    return create_handle(params, width, height, true, out);
+}
+
+size_t volume_bytes(const ds_handle* h) { return (h->values_bytes + 255) / 256 * 256 + h->costs_bytes; }
+
+void bind_volumes(ds_handle* h, void* base) {
+    h->d_values = base;
+    h->d_costs = h->costs_bytes ? static_cast<uint8_t*>(base) + (h->values_bytes + 255) / 256 * 256 : nullptr;
+}
+
+int bind_rectification(ds_handle* h, float* const maps[4], int map_w, int map_h, int raw_w, int raw_h) {
+    const bool same = map_w == h->w && map_h == h->h;
+    const bool twice = map_w == 2 * h->w && map_h == 2 * h->h;
+    if (!same && !twice) return h->fail(DS_INVALID_ARGUMENT, "remap resolution must be the stereo resolution or twice it");
+    if (raw_w < 2 || raw_h < 2 || raw_w > 16384 || raw_h > 16384) return h->fail(DS_INVALID_ARGUMENT, "raw size out of range");
+    return guarded(h, [&]() -> int {
+        if (!h->maps_external) {
+            for (auto*& p : h->d_map)
+                if (p) cudaFree(p), h->bytes -= static_cast<size_t>(h->map_w) * h->map_h * 4;
+        }
+        for (int i = 0; i < 4; ++i) h->d_map[i] = maps[i];
+        h->maps_external = true;
+        if (h->raw_w != raw_w || h->raw_h != raw_h) {
+            for (auto*& p : h->d_raw) {
+                if (p) {
+                    cudaFree(p);
+                    h->bytes -= static_cast<size_t>(h->raw_w) * h->raw_h;
+                    p = nullptr;
+                }
+            }
+            for (auto*& p : h->d_raw) p = h->alloc<uint8_t>(static_cast<size_t>(raw_w) * raw_h);
+        }
+        h->map_w = map_w;
+        h->map_h = map_h;
+        h->raw_w = raw_w;
+        h->raw_h = raw_h;
+        h->have_rect = true;
+        return DS_OK;
+    });
+}
+
+void input_buffers(ds_handle* h, bool raw, uint8_t* out[2]) {
+    for (int s = 0; s < 2; ++s) out[s] = raw ? h->d_raw[s] : h->d_rect[s];
+}
+
+ds_outputs device_outputs(ds_handle* h) { return internal_outputs(h); }
+
+int input_width(const ds_handle* h, bool raw) { return raw ? h->raw_w : h->w; }
+int input_height(const ds_handle* h, bool raw) { return raw ? h->raw_h : h->h; }
+
+}  // namespace ds
+
+extern "C" {
+
+DS_API void ds_default_params(ds_stereo_params* p) {
+    if (!p) return;
+    *p = ds_stereo_params{};
+    p->pyramid_levels = 0;
+    p->sgm.min_disparity = 0;
+    p->sgm.num_disparities = 64;
+    p->sgm.census_radius_x = 2;
+    p->sgm.census_radius_y = 2;
+    p->sgm.p1 = 8;
+    p->sgm.p2 = 96;
+    p->sgm.adaptive_p2 = 1;
+    p->sgm.eight_paths = 0;
+    p->sgm.slant_steps = 1;
+    p->sgm.uniqueness = 0.9f;
+    p->sgm.lr_max_diff = 1;
+    p->subpixel = 1;
+    p->median = 1;
+}
+
+DS_API const char* ds_last_global_error(void) { return g_error.c_str(); }
+
+DS_API int ds_create(const ds_stereo_params* params, int width, int height, ds_handle** out) {
+    return create_handle(params, width, height, false, out);
+}
+
 DS_API void ds_destroy(ds_handle* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
@@ -702,14 +793,15 @@ DS_API int ds_set_rectification(ds_handle* h, const float* lx, const float* ly, 
     if (raw_w < 2 || raw_h < 2 || raw_w > 16384 || raw_h > 16384) return h->fail(DS_INVALID_ARGUMENT, "raw size out of range");
     return guarded(h, [&]() -> int {
         const size_t n = static_cast<size_t>(map_w) * map_h;
-        if (h->map_w != map_w || h->map_h != map_h) {
+        if (h->maps_external || h->map_w != map_w || h->map_h != map_h) {
             for (auto*& p : h->d_map) {
-                if (p) {
+                if (p && !h->maps_external) {
                     cudaFree(p);
                     h->bytes -= static_cast<size_t>(h->map_w) * h->map_h * 4;
-                    p = nullptr;
                 }
+                p = nullptr;
             }
+            h->maps_external = false;
             for (auto*& p : h->d_map) p = h->alloc<float>(n);
         }
         if (h->raw_w != raw_w || h->raw_h != raw_h) {
@@ -1014,6 +1106,7 @@ struct ds_batch {
     dsk::WtaArgs* d_wta = nullptr;
     dsk::PostArgs* d_post = nullptr;
     struct Micro {
+        std::vector<int> pairs;  // heaviest first
         BatchGroup g_rect, g_post;
         std::vector<BatchGroup> g_census, g_costs, g_paths, g_wta;
         int launches() const {
@@ -1021,6 +1114,8 @@ struct ds_batch {
         }
     };
     std::vector<Micro> micro;  // pairs in micro-batches run through all stages back to back
+    std::vector<void*> volumes;  // shared cost / path-value volumes, one per (branch, position) slot
+    size_t volume_bytes = 0;
     int micro_batch = 1, branches = 4;  // best measured for 1280x1024, D=128 on B200
     std::vector<cudaStream_t> branch_st;
     std::vector<cudaEvent_t> fork_join;
@@ -1046,9 +1141,13 @@ void batch_release(ds_batch* b) {
     if (b->graph) cudaGraphDestroy(b->graph);
     for (auto e : b->ev)
         if (e) cudaEventDestroy(e);
+    for (auto* p : b->volumes)
+        if (p) cudaFree(p);
     for (auto* h : b->h) {
         if (!h) continue;
         for (auto*& p : h->d_map) p = nullptr;  // the maps belong to the batch's calibrations
+        h->d_values = nullptr;                  // and the volumes to its slots
+        h->d_costs = nullptr;
         release(h);
         delete h;
     }
@@ -1194,7 +1293,43 @@ void batch_plan(ds_batch* b) {
     for (int first = 0; first < n; first += mb) {
         b->micro.emplace_back();
         std::vector<int> order(all.begin() + first, all.begin() + std::min(n, first + mb));
+        b->micro.back().pairs = order;
         batch_plan_micro(b, b->micro.back(), order);
+    }
+}
+
+// Volumes shared between pairs that never run at the same time: micro-batch i runs on branch i % nb
+// after micro-batch i - nb has finished all its stages (stream order), so its j-th pair can reuse the
+// cost and path-value volumes of micro-batch i - nb's j-th pair. Slot (branch, j) is sized for the
+// largest pair it serves.
+void batch_bind_volumes(ds_batch* b) {
+    const int nm = static_cast<int>(b->micro.size());
+    const int nb = std::max(1, std::min(b->branches, nm));
+    std::vector<std::vector<int>> slots;  // pairs per slot
+    for (int i = 0; i < nm; ++i) {
+        const auto& ps = b->micro[i].pairs;
+        for (size_t j = 0; j < ps.size(); ++j) {
+            const size_t slot = static_cast<size_t>(i % nb) * static_cast<size_t>(b->micro_batch) + j;
+            if (slot >= slots.size()) slots.resize(slot + 1);
+            slots[slot].push_back(ps[j]);
+        }
+    }
+    for (const auto& ps : slots) {
+        if (ps.empty()) continue;
+        size_t vb = 0, cb = 0;
+        for (int p : ps) {
+            vb = std::max(vb, (b->h[p]->values_bytes + 255) / 256 * 256);
+            cb = std::max(cb, b->h[p]->costs_bytes);
+        }
+        void* mem = nullptr;
+        DS_CUDA(cudaMalloc(&mem, vb + cb));
+        b->volumes.push_back(mem);
+        b->volume_bytes += vb + cb;
+        b->bytes += vb + cb;
+        for (int p : ps) {
+            b->h[p]->d_values = mem;
+            b->h[p]->d_costs = b->h[p]->costs_bytes ? static_cast<uint8_t*>(mem) + vb : nullptr;
+        }
     }
 }
 
@@ -1369,7 +1504,7 @@ DS_API int ds_batch_create(const ds_pair_desc* pairs, int n, int n_calib, const 
             break;
         }
         ds_handle* h = nullptr;
-        rc = ds_create(&d.params, d.width, d.height, &h);
+        rc = create_handle(&d.params, d.width, d.height, true, &h);
         if (rc != DS_OK) {
             g_error = "pair " + std::to_string(i) + ": " + g_error;
             break;
@@ -1406,6 +1541,7 @@ DS_API int ds_batch_create(const ds_pair_desc* pairs, int n, int n_calib, const 
             b->fork_join.assign(b->branches + 1, nullptr);
             for (auto& e : b->fork_join) DS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
             batch_plan(b);
+            batch_bind_volumes(b);
             return DS_OK;
         });
     }
@@ -1555,6 +1691,13 @@ DS_API int ds_batch_launches_per_run(const ds_batch* b) {
     int n = 0;
     for (const auto& m : b->micro) n += m.launches();
     return n;
+}
+
+DS_API int ds_batch_get_options(const ds_batch* b, ds_batch_options* out) {
+    if (!b || !out) return DS_INVALID_ARGUMENT;
+    out->micro_batch = b->micro_batch;
+    out->branches = b->branches;
+    return DS_OK;
 }
 
 }  // extern "C"

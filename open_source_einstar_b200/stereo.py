@@ -304,7 +304,7 @@ class CudaStereo:
         return {k: getattr(c, k) for k, _ in c._fields_}
 
     def profile(self, on: bool = True) -> None:
-        """Per-stage CUDA events for every frame (stages: rectify, census, paths, wta+lr, median+outputs)."""
+        """Per-stage CUDA events for every frame (stages: STAGE_NAMES)."""
         self._check(N.lib().ds_profile_enable(self._h, int(bool(on))))
 
     def profile_collect(self, max_frames: int = 4096) -> np.ndarray:
@@ -316,8 +316,8 @@ class CudaStereo:
 
 
 CUDA_STREAM_LEGACY = 1  # (cudaStream_t)0x1
-STAGES = 5
-STAGE_NAMES = ("rectify", "census", "paths", "wta_lr", "median_out")
+STAGES = 6
+STAGE_NAMES = ("rectify", "census", "costs", "paths", "wta_lr", "median_out")
 
 
 def kernel_launches() -> int:

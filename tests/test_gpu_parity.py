@@ -159,6 +159,28 @@ def test_device_entry_matches_host_entry(cuda, golden):
     assert np.array_equal(out["disparity_u16"].cpu().numpy().view(np.uint16), host.disparity_u16)
 
 
+def test_stage_profile(cuda, golden):
+    """Per-frame stage times (the reference's per-stage GPU profile): one row per frame, the cost stage
+    empty when the path kernels recompute costs, and profiling leaves the results unchanged."""
+    from open_source_einstar_b200.stereo import STAGE_NAMES
+    c = golden["plane_sphere_160x128"]
+    p = OracleSgm(**c["params"])
+    with _stereo(p, 160, 128) as s:
+        s.set_kernel_config(1, 16, materialize_costs=True)
+        s.profile(True)
+        outs = [s.compute(c["left"], c["right"]) for _ in range(3)]
+        rows = s.profile_collect()
+        s.set_kernel_config(1, 16, materialize_costs=False)
+        outs.append(s.compute(c["left"], c["right"]))
+        rows2 = s.profile_collect()
+    assert rows.shape == (3, len(STAGE_NAMES)) and rows2.shape == (1, len(STAGE_NAMES))
+    costs, paths = STAGE_NAMES.index("costs"), STAGE_NAMES.index("paths")
+    assert (rows >= 0).all() and (rows[:, costs] > 0).all() and (rows[:, paths] > 0).all()
+    assert rows2[0, costs] < 0.01 and rows2[0, paths] > 0
+    for o in outs:
+        assert same_bits(o.disparity, c["disparity"])
+
+
 def test_strided_host_images(cuda, golden):
     c = golden["plane_sphere_160x128"]
     p = OracleSgm(**c["params"])
@@ -275,8 +297,10 @@ def test_batch_matches_per_pair_runs(cuda, port):
                     s.set_point_params(d.geometry, d.min_depth, d.max_depth)
                 res = s.compute(l, r)
         want.append(res)
+    volume_bytes = []
     for micro_batch, branches in ((len(descs), 1), (0, 0)):  # all pairs per launch; the default schedule
         b = StereoBatch(descs, n_calib=2, micro_batch=micro_batch, branches=branches)
+        volume_bytes.append(b.device_bytes)
         for ci, ((mlx, mly), (mrx, mry)), w, h in [(ci, v[0], v[1], v[2]) for ci, v in calibs.items()]:
             b.set_rectification(ci, RemapTable(mlx, mly), RemapTable(mrx, mry), w, h)
         dev_in, dev_out = [], []
@@ -309,3 +333,5 @@ def test_batch_matches_per_pair_runs(cuda, port):
         if branches == 1:  # one persistent launch per stage and kernel variant for all pairs
             assert b.launches_per_run < 5 * len(descs) // 2
         b.close()
+    # micro-batches that run one after another on a branch share their cost and path-value volumes
+    assert volume_bytes[1] < volume_bytes[0]
