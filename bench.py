@@ -189,6 +189,208 @@ def run_reference(args, world, rank):
     return 0
 
 
+# ---- serving workload: Poisson arrivals of mixed frames through the request server ---------------------------
+SERVE_SIZES = (((1280, 1024), 0.7), ((960, 768), 0.2), ((640, 512), 0.1))
+SERVE_RIGS = ({"f": 1100.0, "baseline": 60.0, "k1": -0.08, "k2": 0.02, "yaw_deg": 1.5},
+              {"f": 1000.0, "baseline": 55.0, "k1": -0.06, "k2": 0.015, "yaw_deg": 1.2},
+              {"f": 1200.0, "baseline": 65.0, "k1": -0.10, "k2": 0.03, "yaw_deg": 1.8},
+              {"f": 1050.0, "baseline": 50.0, "k1": -0.07, "k2": 0.02, "yaw_deg": 1.0})
+SERVE_D = (96, 128)
+
+
+def serving_calibrations(dev):
+    """4 synthetic rigs x 3 sizes: raw speckle pairs of boxes/cylinders at 200-600 mm with their remap tables."""
+    from open_source_einstar_b200 import synth
+    cal = []
+    for r, rig in enumerate(SERVE_RIGS):
+        for s, ((w, h), _) in enumerate(SERVE_SIZES):
+            sc = w / 1280.0
+            pr = synth.raw_objects_pair(seed=500 + 3 * r + s, width=w, height=h, f=rig["f"] * sc, baseline=rig["baseline"],
+                                        k1=rig["k1"], k2=rig["k2"], yaw_deg=rig["yaw_deg"], num_disparities=128,
+                                        device=dev)
+            cal.append((r, s, w, h, pr))
+    return cal
+
+
+def serving_requests(cal, n, seed):
+    """n request descriptors: rig uniform, size 70/20/10 %, D in {96, 128}; pinned inputs and outputs."""
+    from open_source_einstar_b200 import SgmParams, StereoParams
+    from open_source_einstar_b200.serving import pinned_copy, pinned_empty
+    rng = np.random.default_rng(seed)
+    pinned = {}
+    reqs = []
+    for i in range(n):
+        r = int(rng.integers(len(SERVE_RIGS)))
+        s = int(rng.choice(len(SERVE_SIZES), p=[p for _, p in SERVE_SIZES]))
+        d = int(rng.choice(SERVE_D))
+        ci = 3 * r + s
+        _, _, w, h, pr = cal[ci]
+        if ci not in pinned:
+            pinned[ci] = (pinned_copy(pr.left), pinned_copy(pr.right))
+        sp = StereoParams(sgm=SgmParams(min_disparity=pr.min_disparity, num_disparities=d))
+        reqs.append({"left": pinned[ci][0], "right": pinned[ci][1], "width": w, "height": h, "params": sp, "calib": ci,
+                     "outputs": {"disparity_u16": pinned_empty((h, w), np.uint16), "depth": pinned_empty((h, w), np.float32)},
+                     "px_d": w * h * d})
+    return reqs
+
+
+def run_serving(args, world, rank, local):
+    """Poisson arrivals at each rate for --duration seconds through StereoServer (ds_server_*): latency
+    p50/p99/p99.9 from submit to results in host memory, beside frames/s. One GPU; replicas beyond."""
+    import torch
+    from open_source_einstar_b200 import RectifiedGeometry, RemapTable
+    from open_source_einstar_b200.serving import StereoServer, latency_summary, poisson_arrivals, replay
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    cal = serving_calibrations(dev)
+    reqs = serving_requests(cal, 512, seed=11 + rank)
+    srv = StereoServer(volume_budget_bytes=40 << 30, max_slots=args.slots)
+    for ci, (r, s, w, h, pr) in enumerate(cal):
+        (lx, ly), (rx, ry) = pr.maps
+        srv.add_calibration(ci, RemapTable(lx, ly), RemapTable(rx, ry), w, h,
+                            RectifiedGeometry(pr.f, 0, 0, pr.baseline, pr.cx_offset), 150.0, 700.0)
+    from open_source_einstar_b200 import SgmParams, StereoParams
+    for ci, (r, s, w, h, pr) in enumerate(cal[:3]):  # every (size, D) kind, all slots, before the clock starts
+        for d in SERVE_D:
+            srv.reserve(w, h, StereoParams(sgm=SgmParams(min_disparity=pr.min_disparity, num_disparities=d)), ci,
+                        args.slots)
+    replay(srv, reqs, poisson_arrivals(480.0, 0.5, seed=99))  # warm-up
+    clk = ClockSampler(local).__enter__()
+    results = []
+    for k, rate in enumerate(args.rates):
+        arr = poisson_arrivals(rate, args.duration, seed=100 + k)
+        comps, wall = replay(srv, reqs, arr)
+        bad = [c for c in comps if not c.ok]
+        if bad:
+            raise SystemExit(f"{len(bad)} frames failed (status {bad[0].status})")
+        lat = [c.latency_ms for c in comps]
+        pxd = sum(reqs[c.tag % len(reqs)]["px_d"] for c in comps)
+        summ = latency_summary(lat, wall)
+        summ.update({"rate_hz": rate, "seconds": args.duration, "gpix_disp_per_s": pxd / wall / 1e9,
+                     "gpu_ms_p50": float(np.percentile([c.gpu_ms for c in comps], 50)),
+                     "queue_ms_p99": float(np.percentile([c.queue_ms for c in comps], 99))})
+        results.append(summ)
+    clk.__exit__(None, None, None)
+    st = srv.stats()
+    srv.close()
+    if rank == 0:
+        line = {"metric": "serving frame latency p50/p99/p99.9 (ms) beside frames/s, Poisson arrivals",
+                "workload": "serving", "unit": "ms", "higher_is_better": False, "n_gpus": world,
+                "value": max(r["p99_ms"] for r in results), "value_is": "worst p99 latency over the rates",
+                "rates": results, "dtype": "u8", "data": "synthetic",
+                "config": {"workload": "Poisson arrivals; sizes 70 % 1280x1024, 20 % 960x768, 10 % 640x512 (raw pairs, "
+                                       "GPU remap); D in {96, 128}; 4 resident synthetic rigs x 3 sizes; 40 GB volume "
+                                       "budget; latency = submit -> u16 disparity + depth in pinned host memory",
+                           "slots": args.slots, "parallelism": f"replicas x{world}"},
+                "server": {"peak_running": st["peak_running"], "slots": st["slots"],
+                           "volume_bytes": st["volume_bytes"], "device_bytes": st["device_bytes"]},
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---- uneven batch: 64 rectified pairs of three sizes and four disparity ranges in one graph replay -----------
+def run_batch64(args, world, rank, local):
+    """64 pairs (24 x 640x512, 24 x 1280x1024, 16 x 960x768; D from {64, 96, 128, 192}; each its own
+    calibration) as one StereoBatch graph replay with autotuned kernels and schedule, against the same
+    pairs launched per frame (one handle per pair, back to back on one stream). Bit-exact check first."""
+    import torch
+    from open_source_einstar_b200 import (CudaStereo, PairDesc, RectifiedGeometry, SgmParams, StereoBatch, StereoParams,
+                                          synth)
+    from open_source_einstar_b200.autotune import Autotuner, FrameKind, tune_batch_schedule
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pairs = synth.batch_pairs(64, seed=rank, device=dev)
+    tuner = Autotuner()
+    descs, handles, ins, outs = [], [], [], []
+    for pr in pairs:
+        h, w = pr.left.shape
+        sp = StereoParams(sgm=SgmParams(min_disparity=pr.min_disparity, num_disparities=pr.num_disparities))
+        kcfg = tuner.tune(FrameKind.of(w, h, sp))                  # per-frame path (fused pairs allowed)
+        bcfg = tuner.tune(FrameKind.of(w, h, sp), fused_ok=False)  # batched path
+        geom = RectifiedGeometry(pr.f, 0, 0, pr.baseline, 0.0)
+        descs.append(PairDesc(w, h, sp, geometry=geom, kernel=bcfg))
+        s = CudaStereo.create(sp, w, h)
+        from open_source_einstar_b200.autotune import apply
+        apply(s, kcfg)
+        s.set_point_params(geom, 150.0, 700.0)
+        handles.append(s)
+        ins.append((torch.from_numpy(pr.left).to(dev), torch.from_numpy(pr.right).to(dev)))
+        outs.append({"disparity_u16": torch.empty((h, w), dtype=torch.int16, device=dev),
+                     "depth": torch.empty((h, w), dtype=torch.float32, device=dev)})
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    px_d = sum(p.left.shape[0] * p.left.shape[1] * p.num_disparities for p in pairs)
+    formula = sum(algorithmic_bytes(p.left.shape[1], p.left.shape[0], p.num_disparities, P, raw=False) for p in pairs)
+
+    def per_frame():
+        for s, (l, r), o in zip(handles, ins, outs):
+            s.compute_device(l, r, o, stream=stream)
+
+    def make_batch(mb, br):
+        b = StereoBatch(descs, micro_batch=mb, branches=br)
+        for i, ((l, r), o) in enumerate(zip(ins, bouts)):
+            b.bind(i, l, r, o)
+        return b
+
+    def time_run(b):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.run(stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    bouts = [{k: torch.empty_like(v) for k, v in o.items()} for o in outs]
+    (mb, br), sched = tune_batch_schedule(make_batch, time_run, len(descs))
+    batch = make_batch(mb, br)
+    for _ in range(args.warmup):
+        per_frame()
+        batch.run(stream=stream)
+    torch.cuda.synchronize(dev)
+    for i, (o, bo) in enumerate(zip(outs, bouts)):
+        if not (torch.equal(o["disparity_u16"], bo["disparity_u16"]) and torch.equal(o["depth"], bo["depth"])):
+            raise SystemExit(f"pair {i}: batched and per-pair outputs differ")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk = ClockSampler(local).__enter__()
+    e0.record(stream)
+    for _ in range(args.steps):
+        per_frame()
+    e1.record(stream)
+    e1.synchronize()
+    pf_ms = e0.elapsed_time(e1) / args.steps
+    e0.record(stream)
+    for _ in range(args.steps):
+        batch.run(stream=stream)
+    e1.record(stream)
+    e1.synchronize()
+    b_ms = e0.elapsed_time(e1) / args.steps
+    clk.__exit__(None, None, None)
+    hbm, hbm_kind = peaks()
+    line = {"metric": "batched SGM Gpix*disp/s, 64 uneven pairs in one graph replay vs per-frame launches",
+            "workload": "batch64", "value": px_d / (b_ms * 1e-3) / 1e9, "unit": UNIT, "higher_is_better": True,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": b_ms,
+            "per_frame": {"value": px_d / (pf_ms * 1e-3) / 1e9, "ms_per_step": pf_ms},
+            "batched_over_per_frame": pf_ms / b_ms,
+            "pipeline_frac": formula / (b_ms * 1e-3) / 1e9 / hbm, "peak_gbs": hbm, "peak_kind": hbm_kind,
+            "pipeline_formula_bytes": formula,
+            "schedule": {"micro_batch": mb, "branches": br,
+                         "tried_ms": {f"{k[0]}x{k[1]}": v for k, v in sorted(sched.items())}},
+            "launches_per_run": batch.launches_per_run, "device_bytes": batch.device_bytes,
+            "kernels": sorted({json.dumps(d.kernel, sort_keys=True) for d in descs}),
+            "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "24 x 640x512, 24 x 1280x1024, 16 x 960x768 rectified plane+sphere speckle pairs, "
+                                   "D from {64, 96, 128, 192}, f 800-1200 px, baseline 50-70 mm; 4-path SGM, WTA, "
+                                   "L-R, median, u16 + depth", "parallelism": f"replicas x{world}"},
+            "clocks": clk.summary()}
+    batch.close()
+    for s in handles:
+        s.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -199,10 +401,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-budget", type=float, default=150.0, help="seconds of timed reference work at most")
     ap.add_argument("--kernel-config", default="", help="R,SEG,MATERIALIZE override (default: the library's choice)")
+    ap.add_argument("--workload", default="frames", choices=["frames", "serving", "batch64"],
+                    help="frames: the 1280x1024 D=128 throughput line (default); serving: the request-server latency run")
+    ap.add_argument("--duration", type=float, default=20.0, help="serving: seconds of arrivals per rate")
+    ap.add_argument("--rates", type=float, nargs="+", default=[120.0, 240.0, 480.0], help="serving: arrival rates (Hz)")
+    ap.add_argument("--slots", type=int, default=8, help="serving: frames on the GPU at once")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    if args.workload == "serving":
+        return run_serving(args, world, rank, local)
+    if args.workload == "batch64":
+        return run_batch64(args, world, rank, local)
 
     import torch
     from open_source_einstar_b200 import (CudaStereo, PairDesc, RectifiedGeometry, RemapTable, SgmParams, StereoBatch,

@@ -81,7 +81,7 @@ struct ds_handle {
     void* d_census[2] = {nullptr, nullptr};    // padded census: (y, x) at y * cpitch + x, inside census_raw
     void* census_raw[2] = {nullptr, nullptr};
     int cpitch = 0, cguard = 0;
-    size_t census_bytes = 0;                   // per image, guards included
+    size_t census_bytes = 0;                   // per image, guards included (capacity)
     void* d_S = nullptr;                       // fused pairs: vertical sums and horizontal scratch, inside d_values
     void* d_T = nullptr;
     void* d_values = nullptr;
@@ -92,6 +92,8 @@ struct ds_handle {
     // Volumes (d_values, d_costs) owned by a batch that shares them between pairs run one after another;
     // the handle only sizes them.
     bool external_volumes = false;
+    // Frames of this handle may change min_disparity (set_frame_params): census buffers sized for any.
+    bool any_min_disparity = false;
     float* d_disp_lr = nullptr;
     float* d_out_disp = nullptr;
     float* d_out_conf = nullptr;
@@ -306,11 +308,16 @@ void size_config_buffers(ds_handle* h) {
         const int pitch = (h->w + 2 * guard + 3) / 4 * 4;
         const size_t cw = h->census64 ? 8 : 4;
         const size_t cb = static_cast<size_t>(h->h + 2 * g) * pitch * cw;
-        if (cb != h->census_bytes) {
+        if (cb > h->census_bytes) {  // capacity: a smaller layout reuses the buffers
+            size_t cap = cb;
+            if (h->any_min_disparity) {  // room for the guards of every min_disparity in [-512, 512]
+                const int gmax = (dsk::kMaxDisparities + h->dp + g + 4 + 3) / 4 * 4;
+                cap = std::max(cap, static_cast<size_t>(h->h + 2 * g) * ((h->w + 2 * gmax + 3) / 4 * 4) * cw);
+            }
             for (auto*& p : h->census_raw) free_counted(h, p, h->census_bytes);
             h->census_bytes = 0;
-            for (auto*& p : h->census_raw) p = h->alloc<uint8_t>(cb);
-            h->census_bytes = cb;
+            for (auto*& p : h->census_raw) p = h->alloc<uint8_t>(cap);
+            h->census_bytes = cap;
         }
         h->cguard = guard;
         h->cpitch = pitch;
@@ -628,7 +635,8 @@ __global__ void kb_post(const PostArgs* __restrict__ args, const int* __restrict
 
 namespace {
 
-int create_handle(const ds_stereo_params* params, int width, int height, bool external_volumes, ds_handle** out) {
+int create_handle(const ds_stereo_params* params, int width, int height, bool external_volumes, ds_handle** out,
+                  bool any_min_disparity = false) {
     if (!params || !out) {
         g_error = "null argument";
         return DS_INVALID_ARGUMENT;
@@ -658,6 +666,7 @@ int create_handle(const ds_stereo_params* params, int width, int height, bool ex
         h->s16 = h->wide || 2 * (window + params->sgm.p2) > 255;
         h->cfg.fused = false;  // the fused pairs are selectable (ds_set_kernel_config / autotuner)
         h->external_volumes = external_volumes;
+        h->any_min_disparity = any_min_disparity;
         if (h->ndirs == 4) {
             const int rows_max = static_cast<int>(kMaxSmem / (static_cast<size_t>(width) * 4 * dsk::kHorzWordsPerPixel));
             h->cfg.horz_warps = std::max(1, std::min(4, rows_max / (32 / h->cfg.seg)));
@@ -697,7 +706,7 @@ int validate_params(const ds_stereo_params& params, int width, int height, std::
 }
 
 int create_shared_volume_handle(const ds_stereo_params* params, int width, int height, ds_handle** out) {
-    return create_handle(params, width, height, true, out);
+    return create_handle(params, width, height, true, out, true);
 }
 
 size_t volume_bytes(const ds_handle* h) { return (h->values_bytes + 255) / 256 * 256 + h->costs_bytes; }
@@ -734,6 +743,18 @@ int bind_rectification(ds_handle* h, float* const maps[4], int map_w, int map_h,
         h->raw_w = raw_w;
         h->raw_h = raw_h;
         h->have_rect = true;
+        return DS_OK;
+    });
+}
+
+int set_frame_params(ds_handle* h, const ds_stereo_params& p) {
+    ds_stereo_params a = h->p, b = p;
+    a.sgm.min_disparity = b.sgm.min_disparity = 0;
+    if (std::memcmp(&a, &b, sizeof(a)) != 0) return h->fail(DS_INVALID_ARGUMENT, "frame parameters differ beyond min_disparity");
+    if (p.sgm.min_disparity == h->p.sgm.min_disparity) return DS_OK;
+    return guarded(h, [&]() -> int {
+        h->p.sgm.min_disparity = p.sgm.min_disparity;
+        size_config_buffers(h);  // census guards follow min_disparity; buffers are reused when large enough
         return DS_OK;
     });
 }

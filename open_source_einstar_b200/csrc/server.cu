@@ -59,12 +59,14 @@ struct ShapeKey {
 };
 static_assert(sizeof(ShapeKey) == 2 * sizeof(int) + sizeof(ds_stereo_params), "ShapeKey must have no padding");
 
+// Frames that differ only in min_disparity share a handle (it moves the census guards, not the sizes).
 ShapeKey key_of(int w, int h, const ds_stereo_params& p) {
     ShapeKey k;
     std::memset(&k, 0, sizeof(k));
     k.w = w;
     k.h = h;
     k.p = p;
+    k.p.sgm.min_disparity = 0;
     return k;
 }
 
@@ -211,6 +213,7 @@ Slot* pick_slot(ds_server* s, size_t volume) {
 void launch(ds_server* s, Slot& sl, ds_handle* h, const Calib* c) {
     const ds_request& r = sl.job.r;
     const bool raw = r.calib >= 0;
+    if (const int rc = ds::set_frame_params(h, r.params); rc != DS_OK) throw Failure{rc, ds_last_error(h)};
     ds::bind_volumes(h, sl.volume);
     if (raw) {
         const int rc = ds::bind_rectification(h, c->map, c->map_w, c->map_h, c->raw_w, c->raw_h);

@@ -200,6 +200,7 @@ class Projector:
     cell: float = 3.0
     seed: int = 7
     fill: float = 0.5
+    R: np.ndarray | None = None  # world -> projector rotation (None: axes of the world)
 
 
 @dataclass
@@ -296,6 +297,8 @@ def _pattern(proj: Projector, device):
 def _sample_pattern(grid, proj: Projector, P):
     """Projector pixel of world points P -> bilinear sample of the binary cell grid (0 outside)."""
     pp = P - torch.tensor(proj.position, dtype=torch.float64, device=P.device)
+    if proj.R is not None:
+        pp = pp @ torch.tensor(np.asarray(proj.R, np.float64), device=P.device).T
     z = pp[..., 2]
     u = proj.f * pp[..., 0] / z + proj.width / 2.0
     v = proj.f * pp[..., 1] / z + proj.height / 2.0
@@ -459,3 +462,86 @@ def batch_pairs(n=64, seed=0, device="cpu"):
                                      device=device))
     return out
 
+
+
+# --------------------------------------------------------------------------------------------------
+# offline recording: a handheld orbit around a small object
+
+
+@dataclass
+class Recording:
+    """A synthetic raw IR recording: one rig, one object scene, a smooth handheld orbit of n_frames."""
+    rig: Rig
+    rect: Rectification
+    maps: tuple
+    primitives: list
+    poses: list                  # (R_wc, centre) of the left camera per frame
+    min_disparity: int
+    num_disparities: int
+    seed: int
+
+    @property
+    def n_frames(self) -> int:
+        return len(self.poses)
+
+
+def _look_at(centre: np.ndarray, target: np.ndarray, up=(0.0, -1.0, 0.0)) -> np.ndarray:
+    """World -> camera rotation of a camera at `centre` looking at `target` (camera y points down)."""
+    z = target - centre
+    z = z / np.linalg.norm(z)
+    x = np.cross(z, np.asarray(up, np.float64))
+    x = x / np.linalg.norm(x)
+    y = np.cross(z, x)
+    return np.stack([x, y, z])
+
+
+def recording(n_frames=2000, seed=0, width=1280, height=1024, f=1100.0, baseline=60.0, k1=-0.08, k2=0.02,
+              yaw_deg=1.5, num_disparities=256, standoff=(250.0, 450.0), device="cpu") -> Recording:
+    """A 150 mm object (12 random boxes, cylinders and spheres on a base plane) and a smooth handheld
+    trajectory orbiting it at 250-450 mm. min_disparity brackets the object over the whole orbit."""
+    rng = np.random.default_rng(40_000 + seed)
+    prims: list = [Plane((0.0, 60.0, 0.0), (0.0, -1.0, 0.0))]  # base plane (world y points down)
+    for _ in range(12):
+        c = (float(rng.uniform(-55, 55)), float(rng.uniform(-20, 40)), float(rng.uniform(-55, 55)))
+        kind = int(rng.integers(3))
+        if kind == 0:
+            prims.append(Box(c, rot_axis((0, 1, 0), float(rng.uniform(0, math.pi))),
+                             tuple(float(v) for v in rng.uniform(8, 30, 3))))
+        elif kind == 1:
+            prims.append(Cylinder(c, (0.0, 1.0, 0.0), float(rng.uniform(8, 25)), float(rng.uniform(10, 40))))
+        else:
+            prims.append(Sphere(c, float(rng.uniform(10, 30))))
+    rig = make_rig(width, height, f, baseline, k1=k1, k2=k2, yaw_deg=yaw_deg)
+    rect = compute_rectification(rig)
+    maps = (build_remap(rig.left, rect.R_left, rect, device), build_remap(rig.right, rect.R_right, rect, device))
+    # smooth orbit: azimuth sweeps ~1.5 turns, elevation and standoff drift slowly, plus hand tremor
+    t = np.linspace(0.0, 1.0, n_frames)
+    ph = rng.uniform(0, 2 * math.pi, 4)
+    az = 3.0 * math.pi * t + ph[0]
+    el = np.radians(30.0 + 10.0 * np.sin(2 * math.pi * 1.3 * t + ph[1]))
+    lo, hi = standoff
+    r = lo + (hi - lo) * 0.5 * (1 + np.sin(2 * math.pi * 0.9 * t + ph[2]))
+    tremor = 1.5 * np.stack([np.sin(2 * math.pi * 37 * t + ph[3]), np.cos(2 * math.pi * 29 * t),
+                             np.sin(2 * math.pi * 23 * t)], -1)
+    poses = []
+    for i in range(n_frames):
+        c = np.array([r[i] * math.cos(el[i]) * math.sin(az[i]), -r[i] * math.sin(el[i]),
+                      -r[i] * math.cos(el[i]) * math.cos(az[i])]) + tremor[i]
+        poses.append((_look_at(c, np.array([0.0, 10.0, 0.0])), c))
+    z_far = hi + 110.0
+    mind = int(math.floor(rect.f * rect.baseline / z_far)) - 2
+    return Recording(rig, rect, maps, prims, poses, mind, num_disparities, seed)
+
+
+def recording_frame(rec: Recording, i: int, device="cpu") -> tuple[np.ndarray, np.ndarray]:
+    """The raw (distorted) left and right IR images of frame i; the projector moves with the rig."""
+    R_wl, c_l = rec.poses[i]
+    rig = rec.rig
+    R_wr = rig.R @ R_wl                                   # world -> right camera
+    c_r = c_l + R_wl.T @ (-rig.R.T @ rig.t)               # right centre in the world
+    p_rig = np.array([0.5 * rig.baseline, 15.0, 0.0])     # projector between the cameras, as in the rigs above
+    proj = Projector(tuple(c_l + R_wl.T @ p_rig), f=900.0, seed=1000 + rec.seed, R=R_wl)
+    scene = Scene(rec.primitives, proj)
+    left, _ = render(scene, rig.left, R_wl, tuple(c_l), seed=7 * i + 1, device=device)
+    right, _ = render(scene, rig.right, R_wr, tuple(c_r), seed=7 * i + 2, device=device)
+    return left, right
