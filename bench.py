@@ -391,6 +391,69 @@ def run_batch64(args, world, rank, local):
     return 0
 
 
+# ---- offline re-depth: a raw recording in batches of 128 at D=256, 8 paths, u16 path values -----------------
+def run_offline(args, world, rank, local):
+    """A synthetic handheld recording (150 mm object, 250-450 mm standoff, raw 1280x1024 IR pairs) re-depthed
+    in batches of --offline-batch frames: 8-path SGM, D=256, 16-bit path values. Frames are rendered into
+    pinned host memory first (untimed); the timed run covers host->device copies, the batched graph
+    replays and device->host copies of u16 disparity and depth, double-buffered."""
+    import torch
+    from open_source_einstar_b200 import CudaStereo, RectifiedGeometry, RemapTable, SgmParams, StereoParams, synth
+    from open_source_einstar_b200.autotune import Autotuner, FrameKind
+    from open_source_einstar_b200.offline import OfflineRedepth
+    from open_source_einstar_b200.serving import pinned_empty
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    W_, H_, D_ = 1280, 1024, 256
+    n = args.recording_frames
+    rec = synth.recording(n_frames=n, seed=rank, width=W_, height=H_, num_disparities=D_, device=dev)
+    lefts, rights = pinned_empty((n, H_, W_), np.uint8), pinned_empty((n, H_, W_), np.uint8)
+    for i in range(n):
+        lefts[i], rights[i] = synth.recording_frame(rec, i, device=dev)
+    sp = StereoParams(sgm=SgmParams(min_disparity=rec.min_disparity, num_disparities=D_, eight_paths=True),
+                      wide_costs=True)
+    geom = RectifiedGeometry(rec.rect.f, 0, 0, rec.rect.baseline, rec.rect.cx_offset)
+    kernel = Autotuner().tune(FrameKind.of(W_, H_, sp), fused_ok=False)
+    out_u16 = pinned_empty((n, H_, W_), np.uint16)
+    out_depth = pinned_empty((n, H_, W_), np.float32)
+    with OfflineRedepth(W_, H_, sp, rec.maps, (W_, H_), geom, batch_size=args.offline_batch, kernel=kernel) as off:
+        warm = min(n, 2 * args.offline_batch)
+        off.run(lefts[:warm], rights[:warm], out_u16[:warm], out_depth[:warm])
+        clk = ClockSampler(local).__enter__()
+        st = off.run(lefts, rights, out_u16, out_depth)
+        clk.__exit__(None, None, None)
+        dev_bytes = off.device_bytes
+    # spot check: frames re-depthed alone through the per-frame path are identical
+    (lx, ly), (rx, ry) = rec.maps
+    with CudaStereo.create(sp, W_, H_) as s:
+        s.set_rectification(RemapTable(lx, ly), RemapTable(rx, ry), W_, H_)
+        s.set_point_params(geom, 150.0, 700.0)
+        for i in (0, n // 2, n - 1):
+            r = s.compute_raw(lefts[i], rights[i])
+            if not (np.array_equal(r.disparity_u16, out_u16[i]) and np.array_equal(r.depth.view(np.uint32),
+                                                                                   out_depth[i].view(np.uint32))):
+                raise SystemExit(f"offline frame {i} differs from the per-frame path")
+    hbm, hbm_kind = peaks()
+    ms = st.device_ms
+    formula = algorithmic_bytes(W_, H_, D_, 8, c_b=2, raw=True) * n
+    if rank == 0:
+        line = {"metric": "offline re-depth Gpix*disp/s, 8-path D=256 u16, batches of 128 raw 1280x1024 frames",
+                "workload": "offline", "value": n * W_ * H_ * D_ / (ms * 1e-3) / 1e9, "unit": UNIT,
+                "higher_is_better": True, "n_gpus": world, "frames": n, "batches": st.batches,
+                "frames_per_s": n / (ms * 1e-3), "ms_per_frame": ms / n,
+                "pipeline_frac": formula / (ms * 1e-3) / 1e9 / hbm, "pipeline_formula_bytes_per_frame": formula // n,
+                "peak_gbs": hbm, "peak_kind": hbm_kind, "device_bytes": dev_bytes, "kernel": kernel,
+                "dtype": "u16", "data": "synthetic",
+                "config": {"workload": f"synthetic handheld recording of {n} raw 1280x1024 IR pairs (12-primitive 150 mm "
+                                       "object on a base plane, 250-450 mm standoff, speckle, sigma 2 DN); GPU remap, "
+                                       "8-path SGM D=256 with u16 path values, WTA, L-R, median, u16 + depth; "
+                                       "timed: H2D + batched graph replays + D2H, double-buffered",
+                           "batch": args.offline_batch, "parallelism": f"replicas x{world}"},
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -401,11 +464,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-budget", type=float, default=150.0, help="seconds of timed reference work at most")
     ap.add_argument("--kernel-config", default="", help="R,SEG,MATERIALIZE override (default: the library's choice)")
-    ap.add_argument("--workload", default="frames", choices=["frames", "serving", "batch64"],
+    ap.add_argument("--workload", default="frames", choices=["frames", "serving", "batch64", "offline"],
                     help="frames: the 1280x1024 D=128 throughput line (default); serving: the request-server latency run")
     ap.add_argument("--duration", type=float, default=20.0, help="serving: seconds of arrivals per rate")
     ap.add_argument("--rates", type=float, nargs="+", default=[120.0, 240.0, 480.0], help="serving: arrival rates (Hz)")
-    ap.add_argument("--slots", type=int, default=8, help="serving: frames on the GPU at once")
+    ap.add_argument("--slots", type=int, default=6, help="serving: frames on the GPU at once")
+    ap.add_argument("--recording-frames", type=int, default=256, help="offline: frames of the synthetic recording")
+    ap.add_argument("--offline-batch", type=int, default=128, help="offline: frames per batch")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -414,6 +479,8 @@ def main():
         return run_serving(args, world, rank, local)
     if args.workload == "batch64":
         return run_batch64(args, world, rank, local)
+    if args.workload == "offline":
+        return run_offline(args, world, rank, local)
 
     import torch
     from open_source_einstar_b200 import (CudaStereo, PairDesc, RectifiedGeometry, RemapTable, SgmParams, StereoBatch,

@@ -165,6 +165,19 @@ class Autotuner:
         return cfg
 
 
+_shared: Autotuner | None = None
+_device: str | None = None
+
+
+def tuned_config(width: int, height: int, params, batch: bool = False) -> dict | None:
+    """The tuned configuration of this kind of frame on this GPU from the tables, or None (no tuning)."""
+    global _shared, _device
+    if _shared is None:
+        _shared = Autotuner()
+        _device = Autotuner.device_name()
+    return _shared.lookup(FrameKind.of(width, height, params), _device, fused_ok=not batch)
+
+
 def apply(stereo, cfg: dict) -> None:
     stereo.set_kernel_config(cfg["regs_per_lane"], cfg["lanes_per_line"], bool(cfg["materialize_costs"]),
                              cfg["path_warps_per_block"], cfg["wta_threads"], cfg["prefetch_steps"],

@@ -52,9 +52,17 @@ def _stream_handle(stream):
 
 
 class StereoBatch:
-    def __init__(self, pairs: list[PairDesc], n_calib: int = 0, micro_batch: int = 0, branches: int = 0):
-        """micro_batch / branches: see ds_batch_options (0 = the library's defaults)."""
+    def __init__(self, pairs: list[PairDesc], n_calib: int = 0, micro_batch: int = 0, branches: int = 0,
+                 tuned: bool = True):
+        """micro_batch / branches: see ds_batch_options (0 = the library's defaults). With `tuned`, pairs
+        without a kernel configuration take the autotuner's batched-path entry for their kind of frame."""
         L = N.lib()
+        if tuned:
+            from dataclasses import replace
+
+            from .autotune import tuned_config
+            pairs = [p if p.kernel else replace(p, kernel=tuned_config(p.width, p.height, p.params, batch=True))
+                     for p in pairs]
         arr = (N.PairDescC * len(pairs))(*[p.c() for p in pairs])
         h = C.c_void_p()
         opt = N.BatchOptionsC(int(micro_batch), int(branches))

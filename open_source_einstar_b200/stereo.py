@@ -168,14 +168,22 @@ class CudaStereo:
 
     # --- life cycle ---------------------------------------------------------------------------------
     @classmethod
-    def create(cls, params: StereoParams, width: int, height: int) -> "CudaStereo":
-        """MetalStereo::create (metal_stereo.cpp:108-201): validates and allocates device buffers."""
+    def create(cls, params: StereoParams, width: int, height: int, tuned: bool = True) -> "CudaStereo":
+        """MetalStereo::create (metal_stereo.cpp:108-201): validates and allocates device buffers. With
+        `tuned`, the autotuner's table entry for this kind of frame on this GPU (if any) sets the kernel
+        configuration; results do not depend on it."""
         L = N.lib()
         h = C.c_void_p()
         rc = L.ds_create(C.byref(params.c()), int(width), int(height), C.byref(h))
         if rc != 0:
             raise StereoError(rc, L.ds_last_global_error().decode())
-        return cls(h.value, params, int(width), int(height))
+        s = cls(h.value, params, int(width), int(height))
+        if tuned:
+            from .autotune import apply, tuned_config
+            cfg = tuned_config(width, height, params)
+            if cfg:
+                apply(s, cfg)
+        return s
 
     def close(self) -> None:
         if self._h:
