@@ -283,6 +283,7 @@ void launch_wta(ds_handle* h, cudaStream_t st) {
     a.subpixel = h->p.subpixel ? 1 : 0;
     a.lr_max_diff = h->p.sgm.lr_max_diff;
     a.disp = h->d_disp_lr;
+    a.pair_sums = h->s16 ? 0 : 1;
     DS_CUDA(ds::launch_wta(h->cfg, h->wide, a, h->h, static_cast<size_t>(h->w) * 8, st));
     ++g_launches;
 }
@@ -542,7 +543,25 @@ cudaError_t launch_paths(const KernelCfg& cfg, bool c64, bool wide, const dsk::P
                          cudaStream_t st) {
     DS_BY_R(launch_paths, cfg, c64, wide, a, ndirs, max_lines, st)
 }
-cudaError_t launch_wta(const KernelCfg& cfg, bool wide, const dsk::WtaArgs& a, int rows, size_t smem, cudaStream_t st) {
+// The WTA splits the Dp disparities of a pixel over its own lanes: the fewest lanes (8, 16 or 32) whose
+// slab of 2R disparities has an instantiated R, so that more pixels share a warp's per-pixel work.
+KernelCfg wta_split(const KernelCfg& cfg) {
+    const int dp = cfg.dp();
+    for (int seg : {8, 16, 32}) {
+        if (dp % (2 * seg)) continue;
+        const int r = dp / (2 * seg);
+        if (r == 1 || r == 2 || r == 3 || r == 4 || r == 6 || r == 8) {
+            KernelCfg c = cfg;
+            c.R = r;
+            c.seg = seg;
+            return c;
+        }
+    }
+    return cfg;
+}
+
+cudaError_t launch_wta(const KernelCfg& cfg0, bool wide, const dsk::WtaArgs& a, int rows, size_t smem, cudaStream_t st) {
+    const KernelCfg cfg = wta_split(cfg0);
     DS_BY_R(launch_wta, cfg, wide, a, rows, smem, st)
 }
 cudaError_t launch_costs(const KernelCfg& cfg, bool c64, const dsk::CostArgs& a, cudaStream_t st) {
@@ -558,8 +577,9 @@ cudaError_t launch_paths_batch(const KernelCfg& cfg, bool c64, bool wide, const 
                                cudaStream_t st) {
     DS_BY_R(launch_paths_batch, cfg, c64, wide, args, g, st)
 }
-cudaError_t launch_wta_batch(const KernelCfg& cfg, bool wide, int ndirs, const dsk::WtaArgs* args, const BatchGroupDev& g,
-                             size_t smem, cudaStream_t st) {
+cudaError_t launch_wta_batch(const KernelCfg& cfg0, bool wide, int ndirs, const dsk::WtaArgs* args,
+                             const BatchGroupDev& g, size_t smem, cudaStream_t st) {
+    const KernelCfg cfg = wta_split(cfg0);
     DS_BY_R(launch_wta_batch, cfg, wide, ndirs, args, g, smem, st)
 }
 cudaError_t launch_costs_batch(const KernelCfg& cfg, bool c64, const dsk::CostArgs* args, const BatchGroupDev& g,
@@ -1267,6 +1287,7 @@ void batch_fill_args(ds_batch* b) {
         wa.subpixel = h->p.subpixel ? 1 : 0;
         wa.lr_max_diff = sg.lr_max_diff;
         wa.disp = h->d_disp_lr;
+        wa.pair_sums = h->s16 ? 0 : 1;
         auto& q = b->a_post[i];
         const ds_outputs& o = b->out[i];
         q.disp = h->d_disp_lr;

@@ -107,10 +107,11 @@ cudaError_t horz_seg(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedA
     }                                                                                                                \
     cudaError_t launch_wta_r##R(const KernelCfg& cfg, bool wide, const dsk::WtaArgs& a, int rows, size_t smem,       \
                                 cudaStream_t st) {                                                                   \
-        DS_SEG_SWITCH(R,                                                                                             \
-                      (wide ? wta_t<R, (R <= 4 ? 16 : 32), uint16_t>(cfg, a, rows, smem, st)                         \
-                            : wta_t<R, (R <= 4 ? 16 : 32), uint8_t>(cfg, a, rows, smem, st)),                        \
-                      (wide ? wta_t<R, 32, uint16_t>(cfg, a, rows, smem, st) : wta_t<R, 32, uint8_t>(cfg, a, rows, smem, st))) \
+        if (cfg.seg == 8)                                                                                            \
+            return wide ? wta_t<R, 8, uint16_t>(cfg, a, rows, smem, st) : wta_t<R, 8, uint8_t>(cfg, a, rows, smem, st); \
+        if (cfg.seg == 16)                                                                                           \
+            return wide ? wta_t<R, 16, uint16_t>(cfg, a, rows, smem, st) : wta_t<R, 16, uint8_t>(cfg, a, rows, smem, st); \
+        return wide ? wta_t<R, 32, uint16_t>(cfg, a, rows, smem, st) : wta_t<R, 32, uint8_t>(cfg, a, rows, smem, st); \
     }                                                                                                                \
     cudaError_t launch_costs_r##R(const KernelCfg& cfg, bool c64, const dsk::CostArgs& a, cudaStream_t st) {         \
         DS_SEG_SWITCH(R,                                                                                             \
@@ -241,11 +242,14 @@ cudaError_t bcosts_t(const dsk::CostArgs* args, const BatchGroupDev& g, cudaStre
     }                                                                                                                \
     cudaError_t launch_wta_batch_r##R(const KernelCfg& cfg, bool wide, int ndirs, const dsk::WtaArgs* args,          \
                                       const BatchGroupDev& g, size_t smem, cudaStream_t st) {                        \
-        DS_SEG_SWITCH(R,                                                                                             \
-                      (wide ? bwta_t<R, (R <= 4 ? 16 : 32), uint16_t>(cfg, ndirs, args, g, smem, st)                 \
-                            : bwta_t<R, (R <= 4 ? 16 : 32), uint8_t>(cfg, ndirs, args, g, smem, st)),                \
-                      (wide ? bwta_t<R, 32, uint16_t>(cfg, ndirs, args, g, smem, st)                                  \
-                            : bwta_t<R, 32, uint8_t>(cfg, ndirs, args, g, smem, st)))                                 \
+        if (cfg.seg == 8)                                                                                            \
+            return wide ? bwta_t<R, 8, uint16_t>(cfg, ndirs, args, g, smem, st)                                      \
+                        : bwta_t<R, 8, uint8_t>(cfg, ndirs, args, g, smem, st);                                      \
+        if (cfg.seg == 16)                                                                                           \
+            return wide ? bwta_t<R, 16, uint16_t>(cfg, ndirs, args, g, smem, st)                                     \
+                        : bwta_t<R, 16, uint8_t>(cfg, ndirs, args, g, smem, st);                                     \
+        return wide ? bwta_t<R, 32, uint16_t>(cfg, ndirs, args, g, smem, st)                                         \
+                    : bwta_t<R, 32, uint8_t>(cfg, ndirs, args, g, smem, st);                                         \
     }                                                                                                                \
     cudaError_t launch_costs_batch_r##R(const KernelCfg& cfg, bool c64, const dsk::CostArgs* args,                   \
                                         const BatchGroupDev& g, cudaStream_t st) {                                   \

@@ -139,6 +139,10 @@ template <int SEG>
 __device__ __forceinline__ uint32_t seg_min(uint32_t v, int seg) {
     if constexpr (SEG == 32) {
         return __reduce_min_sync(kFull, v);
+    } else if constexpr (SEG == 8) {  // four segments per warp: one butterfly serves all of them
+        v = min(v, __shfl_xor_sync(kFull, v, 4));
+        v = min(v, __shfl_xor_sync(kFull, v, 2));
+        return min(v, __shfl_xor_sync(kFull, v, 1));
     } else {
         const uint32_t r0 = __reduce_min_sync(kFull, seg == 0 ? v : 0xFFFFFFFFu);
         const uint32_t r1 = __reduce_min_sync(kFull, seg == 1 ? v : 0xFFFFFFFFu);
@@ -292,7 +296,8 @@ __global__ void __launch_bounds__(256) k_paths(PathArgs a) {
 // reference's u16 sums, wrap included); left WTA = segment min of (cost << 16 | k) keys (first strict
 // minimum), best non-adjacent cost by a second reduction, uniqueness as a float compare, parabola from
 // the neighbours' costs. Right WTA: every candidate (x, k) offers its key to right pixel x - min - k by
-// a shared-memory atomicMin, which leaves the first strict minimum along that diagonal.
+// a shared-memory atomicMin, which leaves the first strict minimum along that diagonal. Warps whose two
+// pixels are interior (every disparity has a right column) skip the per-element range tests.
 
 struct WtaArgs {
     const void* values;
@@ -303,6 +308,9 @@ struct WtaArgs {
     int subpixel;
     int lr_max_diff;
     float* disp;  // L-R checked
+    // u8 path values with 2 (window + P2) <= 255: two directions add as whole 32-bit words (no carry
+    // crosses a byte), halving the unpacking work. 0 for the general path.
+    int pair_sums;
 };
 
 __device__ __forceinline__ float parabola(float cm, float c0, float cp) {  // stereo.cpp:92-96
@@ -326,19 +334,31 @@ __device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
     constexpr int NV = 2 * R;
     constexpr int VB = NV * static_cast<int>(sizeof(ST));
     constexpr int VW = chunk_words<VB>();
+    constexpr uint32_t kEmpty = 0xFFFFFFFFu;
     extern __shared__ uint32_t smem[];
     uint32_t* rkey = smem;                                // [w]
     float* dleft = reinterpret_cast<float*>(smem + a.w);  // [w]
     const int y = bx;
     const int lane = threadIdx.x & 31, seg = lane / SEG, sl = lane % SEG;
     const int warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (int i = threadIdx.x; i < a.w; i += blockDim.x) rkey[i] = 0xFFFFFFFFu;
+    for (int i = threadIdx.x; i < a.w; i += blockDim.x) rkey[i] = kEmpty;
     __syncthreads();
 
     const ST* __restrict__ vals = static_cast<const ST*>(a.values);
     const int k0 = sl * NV;
     const int per_warp = 32 / SEG;
     const int stride = nwarps * per_warp;
+    // Per register r: the (k, k + 1) index pair of the keys, and masks of the disparities >= nd (padding
+    // of the lane slabs): full keys and 16-bit halves.
+    uint32_t kk[R], pada[R], padb[R], padh[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int ka = k0 + 2 * r;
+        kk[r] = static_cast<uint32_t>(ka) | (static_cast<uint32_t>(ka + 1) << 16);
+        pada[r] = ka >= a.nd ? kEmpty : 0u;
+        padb[r] = ka + 1 >= a.nd ? kEmpty : 0u;
+        padh[r] = (pada[r] & 0xFFFFu) | (padb[r] & 0xFFFF0000u);
+    }
     // Double buffer: the next pixel's chunks are in flight while this one is reduced.
     uint32_t nxt[NDIRS][VW];
     auto fetch = [&](int xb) {
@@ -354,44 +374,88 @@ __device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
         const bool live = x < a.w;
         const int xc = live ? x : a.w - 1;
         uint32_t tot[R];
+        bool paired = false;
+        if constexpr (sizeof(ST) == 1) {
+            if (a.pair_sums) {
+                uint32_t ps[VW];
 #pragma unroll
-        for (int r = 0; r < R; ++r) tot[r] = 0u;
+                for (int d = 0; d < NDIRS; d += 2) {
 #pragma unroll
-        for (int d = 0; d < NDIRS; ++d) {
-            uint32_t v[R];
-            unpack<ST, NV>(nxt[d], v);
+                    for (int w = 0; w < VW; ++w) ps[w] = nxt[d][w] + nxt[d + 1][w];
+                    uint32_t v[R];
+                    unpack<uint8_t, NV>(ps, v);
 #pragma unroll
-            for (int r = 0; r < R; ++r) tot[r] = vadd2(tot[r], v[r]);
+                    for (int r = 0; r < R; ++r) tot[r] = d == 0 ? v[r] : vadd2(tot[r], v[r]);
+                }
+                paired = true;
+            }
+        }
+        if (!paired) {
+#pragma unroll
+            for (int d = 0; d < NDIRS; ++d) {
+                uint32_t v[R];
+                unpack<ST, NV>(nxt[d], v);
+#pragma unroll
+                for (int r = 0; r < R; ++r) tot[r] = d == 0 ? v[r] : vadd2(tot[r], v[r]);
+            }
         }
         if (xb + stride < a.w) fetch(xb + stride);
         const int lo = max(0, xc - a.min_disp - (a.w - 1));
         const int hi = min(a.nd, xc - a.min_disp + 1);
-        uint32_t kmin = 0xFFFFFFFFu;
+        const int rbase = xc - a.min_disp - k0;  // right column of the lane's first disparity
+        uint32_t key, second;
+        if (__all_sync(kFull, live && lo == 0 && hi == a.nd)) {
+            // Interior pixels (every disparity < nd matches a column of the right row): no per-element
+            // range tests; padding keys are all ones and take part in nothing.
+            uint32_t kmin = kEmpty;
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int ka = k0 + 2 * r;
-            const uint32_t kk = static_cast<uint32_t>(ka) | (static_cast<uint32_t>(ka + 1) << 16);
-            const uint32_t key_a = prmt(kk, tot[r], 0x5410);  // (cost_a << 16) | ka
-            const uint32_t key_b = prmt(kk, tot[r], 0x7632);  // (cost_b << 16) | ka + 1
-            if (live && ka >= lo && ka < hi) {
-                kmin = min(kmin, key_a);
-                atomicMin(&rkey[xc - a.min_disp - ka], key_a);
+            for (int r = 0; r < R; ++r) {
+                const uint32_t key_a = prmt(kk[r], tot[r], 0x5410) | pada[r];  // (cost_a << 16) | ka
+                const uint32_t key_b = prmt(kk[r], tot[r], 0x7632) | padb[r];  // (cost_b << 16) | ka + 1
+                kmin = min(kmin, min(key_a, key_b));
+                if (key_a != kEmpty) atomicMin(&rkey[rbase - 2 * r], key_a);
+                if (key_b != kEmpty) atomicMin(&rkey[rbase - 2 * r - 1], key_b);
             }
-            if (live && ka + 1 >= lo && ka + 1 < hi) {
-                kmin = min(kmin, key_b);
-                atomicMin(&rkey[xc - a.min_disp - ka - 1], key_b);
+            key = seg_min<SEG>(kmin, seg);
+            const int bk = static_cast<int>(key & 0xFFFFu);
+            uint32_t m2 = kEmpty;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int ka = k0 + 2 * r;
+                // disparities within one of bk are not the second minimum (stereo.cpp:420-424)
+                const uint32_t ex = (static_cast<unsigned>(ka - bk + 1) <= 2u ? 0x0000FFFFu : 0u) |
+                                    (static_cast<unsigned>(ka - bk + 2) <= 2u ? 0xFFFF0000u : 0u);
+                m2 = vmin2(m2, tot[r] | padh[r] | ex);
             }
+            second = seg_min<SEG>(hmin2(m2), seg);
+        } else {
+            uint32_t kmin = kEmpty;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int ka = k0 + 2 * r;
+                const uint32_t key_a = prmt(kk[r], tot[r], 0x5410);
+                const uint32_t key_b = prmt(kk[r], tot[r], 0x7632);
+                if (live && ka >= lo && ka < hi) {
+                    kmin = min(kmin, key_a);
+                    atomicMin(&rkey[rbase - 2 * r], key_a);
+                }
+                if (live && ka + 1 >= lo && ka + 1 < hi) {
+                    kmin = min(kmin, key_b);
+                    atomicMin(&rkey[rbase - 2 * r - 1], key_b);
+                }
+            }
+            key = seg_min<SEG>(kmin, seg);
+            const int bk = static_cast<int>(key & 0xFFFFu);
+            uint32_t sec = 0xFFFFu;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int ka = k0 + 2 * r;
+                if (ka >= lo && ka < hi && (ka - bk > 1 || bk - ka > 1)) sec = min(sec, tot[r] & 0xFFFFu);
+                if (ka + 1 >= lo && ka + 1 < hi && (ka + 1 - bk > 1 || bk - ka - 1 > 1)) sec = min(sec, tot[r] >> 16);
+            }
+            second = seg_min<SEG>(sec, seg);
         }
-        const uint32_t key = seg_min<SEG>(kmin, seg);
         const int bk = static_cast<int>(key & 0xFFFFu);
-        uint32_t second = 0xFFFFu;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const int ka = k0 + 2 * r;
-            if (ka >= lo && ka < hi && (ka - bk > 1 || bk - ka > 1)) second = min(second, tot[r] & 0xFFFFu);
-            if (ka + 1 >= lo && ka + 1 < hi && (ka + 1 - bk > 1 || bk - ka - 1 > 1)) second = min(second, tot[r] >> 16);
-        }
-        second = seg_min<SEG>(second, seg);
         const int km = max(bk - 1, 0), kp = min(bk + 1, a.nd - 1);
         const uint32_t vm = __shfl_sync(kFull, pick16<R>(tot, km % NV), km / NV, SEG);
         const uint32_t vp = __shfl_sync(kFull, pick16<R>(tot, kp % NV), kp / NV, SEG);
