@@ -151,7 +151,7 @@ __global__ void __launch_bounds__(256) kb_paths(const PathArgs* __restrict__ arg
             __syncthreads();
             cur = p;
         }
-        paths_body<R, SEG, CW, ST, MAT, PF>(sa, lb % g, lb / g);
+        paths_body<R, SEG, CW, ST, MAT, PF>(sa, sa.p2_table, lb % g, lb / g);
     }
 }
 

@@ -78,6 +78,79 @@ __global__ void __launch_bounds__(256) k_costs(CostArgs a) {
     costs_body<R, SEG, CW>(a, blockIdx.x);
 }
 
+// Row-tiled cost volume: one block per tile of kCostTile pixels of a row. The right census words the
+// tile needs (kCostTile + dp - 1 of them) are staged in shared memory, four times with shifts of 0..3
+// words, so that every thread reads the four words of its four consecutive disparities with one
+// aligned 128-bit load (u32 census). Thread t of a pixel writes the bytes of disparities 4t..4t+3, so
+// a warp stores whole 128-byte lines. Columns outside the right row give invalid_cost
+// (stereo.cpp:366-377).
+constexpr int kCostTile = 64;
+
+// Words per shifted copy (a multiple of 4, so that every copy starts 16-byte aligned).
+__host__ __device__ constexpr int cost_tile_copy_words(int dp) { return (kCostTile + dp + 3 + 3) / 4 * 4; }
+
+template <typename CW>
+__host__ __device__ constexpr size_t cost_tile_smem(int dp) {
+    return sizeof(CW) * (static_cast<size_t>(sizeof(CW) == 4 ? 4 : 1) * cost_tile_copy_words(dp) + kCostTile);
+}
+
+template <typename CW>
+__device__ __forceinline__ void cost_tile_body(const CostArgs& a, int b, CW* sm) {
+    constexpr int NC = sizeof(CW) == 4 ? 4 : 1;  // shifted copies
+    const int tiles = (a.w + kCostTile - 1) / kCostTile;
+    const int y = b / tiles, x0 = (b % tiles) * kCostTile;
+    const int nx = min(kCostTile, a.w - x0);
+    const int r0 = x0 - a.min_disp - (a.dp - 1);  // right column of window slot 0
+    const int nr = nx + a.dp - 1;
+    const int cpy = cost_tile_copy_words(a.dp);
+    CW* sl = sm + NC * cpy;
+    const CW* cl = static_cast<const CW*>(a.census_l) + static_cast<size_t>(y) * a.cpitch;
+    const CW* cr = static_cast<const CW*>(a.census_r) + static_cast<size_t>(y) * a.cpitch;
+    __syncthreads();  // the previous tile's readers are done
+    for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+        const int xr = r0 + i;
+        const CW v = static_cast<unsigned>(xr) < static_cast<unsigned>(a.w) ? __ldg(cr + xr) : CW(0);
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+            if (i - c >= 0) sm[c * cpy + i - c] = v;  // copy c holds word i at i - c
+    }
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) sl[i] = __ldg(cl + x0 + i);
+    __syncthreads();
+    const int tp = a.dp >> 2;  // threads per pixel
+    const int ppp = static_cast<int>(blockDim.x) / tp;
+    const int t = threadIdx.x % tp, pi = threadIdx.x / tp;
+    if (pi >= ppp) return;
+    const uint32_t inv = static_cast<uint32_t>(a.invalid_cost);
+    for (int px = pi; px < nx; px += ppp) {
+        const CW vl = sl[px];
+        const int g = px + a.dp - 4 - 4 * t;  // window slot of disparity 4t + 3; slot g + 3 - j is disparity 4t + j
+        CW wv[4];
+        if constexpr (NC == 4) {
+            const int c = g & 3;
+            const uint4 q = *reinterpret_cast<const uint4*>(sm + c * cpy + g - c);
+            wv[0] = q.x, wv[1] = q.y, wv[2] = q.z, wv[3] = q.w;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) wv[j] = sm[g + j];
+        }
+        uint32_t word = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {  // byte j: disparity 4t + j, right column r0 + g + 3 - j
+            const int xr = r0 + g + 3 - j;
+            const uint32_t cst = static_cast<unsigned>(xr) < static_cast<unsigned>(a.w)
+                                     ? static_cast<uint32_t>(popcount_word<CW>(vl ^ wv[3 - j])) : inv;
+            word |= cst << (8 * j);
+        }
+        *reinterpret_cast<uint32_t*>(a.costs + (static_cast<size_t>(y) * a.w + x0 + px) * a.dp + 4 * t) = word;
+    }
+}
+
+template <typename CW>
+__global__ void __launch_bounds__(256) k_cost_tiles(CostArgs a) {
+    extern __shared__ __align__(16) unsigned char cost_smem[];
+    cost_tile_body<CW>(a, blockIdx.x, reinterpret_cast<CW*>(cost_smem));
+}
+
 // ------------------------------------------------------------------------------------------------
 // Path aggregation (stereo.cpp:44-89, directions and start pixels :382-409).
 //
@@ -151,8 +224,9 @@ __device__ __forceinline__ uint32_t seg_min(uint32_t v, int seg) {
 }
 
 // PF: depth of the register prefetch ring (the inputs of step s + PF are loaded while step s runs).
+// p2: the adaptive-P2 table of `a` in shared memory (it is indexed by the intensity step every step).
 template <int R, int SEG, typename CW, typename ST, bool MAT, int PF>
-__device__ __forceinline__ void paths_body(const PathArgs& a, int bx, int by) {
+__device__ __forceinline__ void paths_body(const PathArgs& a, const int* p2, int bx, int by) {
     constexpr int NV = 2 * R;
     constexpr int LPW = 32 / SEG;  // lines per warp
     constexpr int CWN = chunk_words<NV>();
@@ -186,18 +260,22 @@ __device__ __forceinline__ void paths_body(const PathArgs& a, int bx, int by) {
         any_pad |= pad[r] != 0u;
     }
 
+    // Pixel index of step s: idx0 + s * dstep. Steps past the line's end (the shorter line of a warp's
+    // pair, or a lane without a line) read the line's last pixel; their values are never stored.
+    const int idx0 = y0 * a.w + x0, dstep = dy * a.w + dx, smax = max(len - 1, 0);
     // Prefetch ring: guide intensity and census words (or the cost chunk) of upcoming steps.
     int pI[PF];
     CW pvl[PF];
     CW pvr[PF][MAT ? 1 : NV];
     uint32_t pcw[PF][MAT ? CWN : 1];
     auto fetch = [&](int s, int u) {
-        const int cx = min(max(x0 + s * dx, 0), a.w - 1), cy = min(max(y0 + s * dy, 0), a.h - 1);
-        const size_t row = static_cast<size_t>(cy) * a.w;
-        pI[u] = __ldg(a.guide + row + cx);
+        const int sc = min(s, smax);
+        const int idx = idx0 + sc * dstep;
+        pI[u] = __ldg(a.guide + idx);
         if constexpr (MAT) {
-            ld_chunk<NV, LD_NC>(a.costs + (row + cx) * a.dp + k0, pcw[u]);
+            ld_chunk<NV, LD_NC>(a.costs + static_cast<size_t>(idx) * a.dp + k0, pcw[u]);
         } else {
+            const int cx = x0 + sc * dx, cy = y0 + sc * dy;
             const size_t crow = static_cast<size_t>(cy) * a.cpitch;
             pvl[u] = __ldg(cl + crow + cx);
 #pragma unroll
@@ -222,10 +300,10 @@ __device__ __forceinline__ void paths_body(const PathArgs& a, int bx, int by) {
             }
         }
     };
-    auto store = [&](int x, int y, const uint32_t (&v)[R]) {
+    auto store = [&](int s, const uint32_t (&v)[R]) {
         uint32_t w[chunk_words<VB>()];
         pack<ST, NV>(v, w);
-        st_chunk<VB, true>(out + (static_cast<size_t>(y) * a.w + x) * a.dp + k0, w);
+        st_chunk<VB, true>(out + static_cast<size_t>(idx0 + s * dstep) * a.dp + k0, w);
     };
 
     uint32_t prev[R], c[R];
@@ -242,7 +320,7 @@ __device__ __forceinline__ void paths_body(const PathArgs& a, int bx, int by) {
         lmin = vmin2(lmin, prev[r]);
     }
     uint32_t pm = seg_min<SEG>(hmin2(lmin), seg);
-    if (len > 0) store(x0, y0, prev);
+    if (len > 0) store(0, prev);
 
     int x = x0, y = y0;
     for (int base = 1; base < nsteps; base += PF) {
@@ -257,7 +335,7 @@ __device__ __forceinline__ void paths_body(const PathArgs& a, int bx, int by) {
             if (s + PF < nsteps) fetch(s + PF, u);
             const int dI = I > last_i ? I - last_i : last_i - I;
             last_i = I;
-            const uint32_t jump2 = splat2(pm + static_cast<uint32_t>(a.p2_table[dI >> 3]));
+            const uint32_t jump2 = splat2(pm + static_cast<uint32_t>(p2[dI >> 3]));
             const uint32_t negpm = splat2(0x10000u - pm);
             uint32_t up = __shfl_up_sync(kFull, prev[R - 1], 1, SEG);
             uint32_t dn = __shfl_down_sync(kFull, prev[0], 1, SEG);
@@ -280,14 +358,17 @@ __device__ __forceinline__ void paths_body(const PathArgs& a, int bx, int by) {
             pm = seg_min<SEG>(hmin2(lmin), seg);
 #pragma unroll
             for (int r = 0; r < R; ++r) prev[r] = cur[r];
-            if (s < len) store(x, y, cur);
+            if (s < len) store(s, cur);
         }
     }
 }
 
 template <int R, int SEG, typename CW, typename ST, bool MAT, int PF>
 __global__ void __launch_bounds__(256) k_paths(PathArgs a) {
-    paths_body<R, SEG, CW, ST, MAT, PF>(a, blockIdx.x, blockIdx.y);
+    __shared__ int p2[32];
+    if (threadIdx.x < 32) p2[threadIdx.x] = a.p2_table[threadIdx.x];
+    __syncthreads();
+    paths_body<R, SEG, CW, ST, MAT, PF>(a, p2, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -296,8 +377,8 @@ __global__ void __launch_bounds__(256) k_paths(PathArgs a) {
 // reference's u16 sums, wrap included); left WTA = segment min of (cost << 16 | k) keys (first strict
 // minimum), best non-adjacent cost by a second reduction, uniqueness as a float compare, parabola from
 // the neighbours' costs. Right WTA: every candidate (x, k) offers its key to right pixel x - min - k by
-// a shared-memory atomicMin, which leaves the first strict minimum along that diagonal. Warps whose two
-// pixels are interior (every disparity has a right column) skip the per-element range tests.
+// a shared-memory atomicMin, which leaves the first strict minimum along that diagonal. Candidates are
+// selected by all-ones masks OR-ed into keys and sums, so there are no per-element branches.
 
 struct WtaArgs {
     const void* values;
@@ -349,15 +430,14 @@ __device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
     const int per_warp = 32 / SEG;
     const int stride = nwarps * per_warp;
     // Per register r: the (k, k + 1) index pair of the keys, and masks of the disparities >= nd (padding
-    // of the lane slabs): full keys and 16-bit halves.
-    uint32_t kk[R], pada[R], padb[R], padh[R];
+    // of the lane slabs).
+    uint32_t kk[R], pada[R], padb[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int ka = k0 + 2 * r;
         kk[r] = static_cast<uint32_t>(ka) | (static_cast<uint32_t>(ka + 1) << 16);
         pada[r] = ka >= a.nd ? kEmpty : 0u;
         padb[r] = ka + 1 >= a.nd ? kEmpty : 0u;
-        padh[r] = (pada[r] & 0xFFFFu) | (padb[r] & 0xFFFF0000u);
     }
     // Double buffer: the next pixel's chunks are in flight while this one is reduced.
     uint32_t nxt[NDIRS][VW];
@@ -403,20 +483,33 @@ __device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
         const int lo = max(0, xc - a.min_disp - (a.w - 1));
         const int hi = min(a.nd, xc - a.min_disp + 1);
         const int rbase = xc - a.min_disp - k0;  // right column of the lane's first disparity
-        uint32_t key, second;
+        // Candidate masks (all ones where disparity k is not a candidate of this pixel: outside [lo, hi)
+        // or padding). Interior warps (every k < nd has a right column) take the padding masks as they are.
+        uint32_t ma[R], mb[R];
         if (__all_sync(kFull, live && lo == 0 && hi == a.nd)) {
-            // Interior pixels (every disparity < nd matches a column of the right row): no per-element
-            // range tests; padding keys are all ones and take part in nothing.
-            uint32_t kmin = kEmpty;
+#pragma unroll
+            for (int r = 0; r < R; ++r) ma[r] = pada[r], mb[r] = padb[r];
+        } else {
+            const unsigned span = live ? static_cast<unsigned>(max(hi - lo, 0)) : 0u;
+            const int base = k0 - lo;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                const uint32_t key_a = prmt(kk[r], tot[r], 0x5410) | pada[r];  // (cost_a << 16) | ka
-                const uint32_t key_b = prmt(kk[r], tot[r], 0x7632) | padb[r];  // (cost_b << 16) | ka + 1
-                kmin = min(kmin, min(key_a, key_b));
-                if (key_a != kEmpty) atomicMin(&rkey[rbase - 2 * r], key_a);
-                if (key_b != kEmpty) atomicMin(&rkey[rbase - 2 * r - 1], key_b);
+                ma[r] = static_cast<unsigned>(base + 2 * r) < span ? 0u : kEmpty;
+                mb[r] = static_cast<unsigned>(base + 2 * r + 1) < span ? 0u : kEmpty;
             }
-            key = seg_min<SEG>(kmin, seg);
+        }
+        uint32_t kmin = kEmpty;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const uint32_t key_a = prmt(kk[r], tot[r], 0x5410) | ma[r];  // (cost_a << 16) | ka
+            const uint32_t key_b = prmt(kk[r], tot[r], 0x7632) | mb[r];  // (cost_b << 16) | ka + 1
+            kmin = min(kmin, min(key_a, key_b));
+            if (key_a != kEmpty) atomicMin(&rkey[rbase - 2 * r], key_a);
+            if (key_b != kEmpty) atomicMin(&rkey[rbase - 2 * r - 1], key_b);
+        }
+        const uint32_t key = seg_min<SEG>(kmin, seg);
+        uint32_t second;
+        {
             const int bk = static_cast<int>(key & 0xFFFFu);
             uint32_t m2 = kEmpty;
 #pragma unroll
@@ -425,35 +518,9 @@ __device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
                 // disparities within one of bk are not the second minimum (stereo.cpp:420-424)
                 const uint32_t ex = (static_cast<unsigned>(ka - bk + 1) <= 2u ? 0x0000FFFFu : 0u) |
                                     (static_cast<unsigned>(ka - bk + 2) <= 2u ? 0xFFFF0000u : 0u);
-                m2 = vmin2(m2, tot[r] | padh[r] | ex);
+                m2 = vmin2(m2, tot[r] | (ma[r] & 0x0000FFFFu) | (mb[r] & 0xFFFF0000u) | ex);
             }
             second = seg_min<SEG>(hmin2(m2), seg);
-        } else {
-            uint32_t kmin = kEmpty;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int ka = k0 + 2 * r;
-                const uint32_t key_a = prmt(kk[r], tot[r], 0x5410);
-                const uint32_t key_b = prmt(kk[r], tot[r], 0x7632);
-                if (live && ka >= lo && ka < hi) {
-                    kmin = min(kmin, key_a);
-                    atomicMin(&rkey[rbase - 2 * r], key_a);
-                }
-                if (live && ka + 1 >= lo && ka + 1 < hi) {
-                    kmin = min(kmin, key_b);
-                    atomicMin(&rkey[rbase - 2 * r - 1], key_b);
-                }
-            }
-            key = seg_min<SEG>(kmin, seg);
-            const int bk = static_cast<int>(key & 0xFFFFu);
-            uint32_t sec = 0xFFFFu;
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int ka = k0 + 2 * r;
-                if (ka >= lo && ka < hi && (ka - bk > 1 || bk - ka > 1)) sec = min(sec, tot[r] & 0xFFFFu);
-                if (ka + 1 >= lo && ka + 1 < hi && (ka + 1 - bk > 1 || bk - ka - 1 > 1)) sec = min(sec, tot[r] >> 16);
-            }
-            second = seg_min<SEG>(sec, seg);
         }
         const int bk = static_cast<int>(key & 0xFFFFu);
         const int km = max(bk - 1, 0), kp = min(bk + 1, a.nd - 1);
