@@ -229,7 +229,12 @@ void launch_costs(ds_handle* h, cudaStream_t st) {
     const int window = (2 * sg.census_radius_x + 1) * (2 * sg.census_radius_y + 1);
     dsk::CostArgs c{h->d_census[0], h->d_census[1], h->d_costs, h->w, h->h, h->nd, h->dp, sg.min_disparity, window,
                     h->cpitch};
-    DS_CUDA(ds::launch_costs(h->cfg, h->census64, c, st));
+    const int tiles = (h->w + dsk::kCostTile - 1) / dsk::kCostTile;
+    if (h->census64)
+        dsk::k_cost_tiles<uint64_t><<<h->h * tiles, 256, dsk::cost_tile_smem<uint64_t>(h->dp), st>>>(c);
+    else
+        dsk::k_cost_tiles<uint32_t><<<h->h * tiles, 256, dsk::cost_tile_smem<uint32_t>(h->dp), st>>>(c);
+    DS_CUDA(cudaGetLastError());
     ++g_launches;
 }
 
@@ -635,6 +640,20 @@ __global__ void kb_census(const CensusArgs* __restrict__ args, const int* __rest
         decode3(v - __ldg(prefix + i), __ldg(gx + i), __ldg(gy + i), bx, by, bz);
         stage_args(sa, args, __ldg(pairs + i), cur);
         census_body<W>(sa, bx, by, bz);
+    }
+}
+
+// Cost tiles of all pairs of a group: virtual block = (row, tile) of a pair.
+template <typename W>
+__global__ void __launch_bounds__(256) kb_cost_tiles(const CostArgs* __restrict__ args, const int* __restrict__ pairs,
+                                                     const int* __restrict__ prefix, int n, int total) {
+    extern __shared__ __align__(16) unsigned char cost_smem[];
+    __shared__ CostArgs sa;
+    int cur = -1;
+    for (int v = blockIdx.x; v < total; v += gridDim.x) {
+        const int i = batch_find(prefix, n, v);
+        stage_args(sa, args, __ldg(pairs + i), cur);
+        cost_tile_body<W>(sa, v - __ldg(prefix + i), reinterpret_cast<W*>(cost_smem));
     }
 }
 
@@ -1406,8 +1425,7 @@ void batch_plan_micro(ds_batch* b, ds_batch::Micro& m, const std::vector<int>& o
             });
             g.cfg = c;
             g.c64 = h->census64;
-            const long px = static_cast<long>(h->w) * h->h, per = 8 * (32 / c.seg);
-            add(g, i, static_cast<int>((px + per - 1) / per), 1, 1);
+            add(g, i, h->h * ((h->w + dsk::kCostTile - 1) / dsk::kCostTile), 1, 1);
         }
         {
             BatchGroup& g = find_or_add(m.g_paths, [&](const BatchGroup& x) {
@@ -1466,7 +1484,17 @@ void batch_enqueue_micro(ds_batch* b, const ds_batch::Micro& m, cudaStream_t st,
     }
     mark(2);
     for (const auto& g : m.g_costs) {
-        DS_CUDA(ds::launch_costs_batch(g.cfg, g.c64, b->d_costs, g.dev(), st));
+        const int n = static_cast<int>(g.pairs.size());
+        if (g.c64) {
+            const size_t sm = cost_tile_smem<uint64_t>(g.cfg.dp());
+            kb_cost_tiles<uint64_t><<<grid_of(kb_cost_tiles<uint64_t>, 256, sm, g.total), 256, sm, st>>>(
+                b->d_costs, g.d_pairs, g.d_prefix, n, g.total);
+        } else {
+            const size_t sm = cost_tile_smem<uint32_t>(g.cfg.dp());
+            kb_cost_tiles<uint32_t><<<grid_of(kb_cost_tiles<uint32_t>, 256, sm, g.total), 256, sm, st>>>(
+                b->d_costs, g.d_pairs, g.d_prefix, n, g.total);
+        }
+        DS_CUDA(cudaGetLastError());
         ++g_launches;
     }
     mark(3);
