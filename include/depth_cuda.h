@@ -169,9 +169,10 @@ DS_API int ds_profile_collect(ds_handle* handle, double* stage_ms, int max_frame
 DS_API uint64_t ds_kernel_launches(void);
 
 /* Kernel configuration (no counterpart in the reference; the Metal port picks its SIMD variant at
- * create, metal_stereo.cpp:178-189). A scanline (and a WTA pixel) is run by `lanes_per_line` lanes (16 or
- * 32) holding 2*regs_per_lane disparities each, so lanes_per_line * 2 * regs_per_lane >= num_disparities.
- * Supported: 16 lanes with regs 1..4; 32 lanes with regs 1, 2, 3, 4, 6, 8. materialize_costs: write the
+ * create, metal_stereo.cpp:178-189). A scanline is run by `lanes_per_line` lanes (8, 16 or 32) holding
+ * 2*regs_per_lane disparities each, so lanes_per_line * 2 * regs_per_lane >= num_disparities (the WTA
+ * picks its own split of the same disparities). Supported: 8 lanes with regs 4, 6, 8; 16 lanes with
+ * regs 1..4; 32 lanes with regs 1, 2, 3, 4, 6, 8 (fused pairs: 16 or 32 lanes). materialize_costs: write the
  * matching-cost volume once instead of recomputing costs from the census in every direction. Results are
  * identical for every configuration; only speed differs (the autotuner chooses). */
 typedef struct ds_kernel_config {

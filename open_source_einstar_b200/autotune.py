@@ -32,7 +32,7 @@ from dataclasses import dataclass
 import numpy as np
 
 PACKAGE_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "b200.json")
-SUPPORTED = {16: (1, 2, 3, 4), 32: (1, 2, 3, 4, 6, 8)}
+SUPPORTED = {8: (4, 6, 8), 16: (1, 2, 3, 4), 32: (1, 2, 3, 4, 6, 8)}
 DEFAULT = {"path_warps_per_block": 4, "wta_threads": 256, "prefetch_steps": 8, "fused_pairs": 0,
            "horz_warps_per_block": 4}
 
@@ -75,7 +75,7 @@ def stage_candidates(kind: FrameKind, stage: int, best: dict | None = None, fuse
         for r, seg in tile_shapes(kind.num_disparities):
             for mat in (1, 0):
                 c.append({"regs_per_lane": r, "lanes_per_line": seg, "materialize_costs": mat, **DEFAULT})
-            if fused_ok and not kind.eight_paths:
+            if fused_ok and not kind.eight_paths and seg != 8:
                 c.append({"regs_per_lane": r, "lanes_per_line": seg, "materialize_costs": 0, **DEFAULT,
                           "fused_pairs": 1})
         return c

@@ -528,6 +528,7 @@ void set_global_error(const char* message) { g_error = message ? message : ""; }
 void count_launches(int n) { g_launches += static_cast<uint64_t>(n); }
 
 bool cfg_supported(int R, int seg) {
+    if (seg == 8) return R == 4 || R == 6 || R == 8;
     if (seg == 16) return R == 1 || R == 2 || R == 3 || R == 4;
     if (seg == 32) return R == 1 || R == 2 || R == 3 || R == 4 || R == 6 || R == 8;
     return false;
@@ -1055,7 +1056,8 @@ DS_API int ds_set_kernel_config(ds_handle* h, const ds_kernel_config* c) {
     if (!h) return DS_INVALID_ARGUMENT;
     if (!c) return h->fail(DS_INVALID_ARGUMENT, "null kernel config");
     if (!ds::cfg_supported(c->regs_per_lane, c->lanes_per_line))
-        return h->fail(DS_INVALID_ARGUMENT, "unsupported kernel configuration (lanes per line 16: R 1-4; 32: R 1,2,3,4,6,8)");
+        return h->fail(DS_INVALID_ARGUMENT,
+                       "unsupported kernel configuration (lanes per line 8: R 4,6,8; 16: R 1-4; 32: R 1,2,3,4,6,8)");
     if (c->lanes_per_line * 2 * c->regs_per_lane < h->nd)
         return h->fail(DS_INVALID_ARGUMENT, "kernel configuration holds fewer disparities than num_disparities");
     if (c->path_warps_per_block < 1 || c->path_warps_per_block > 8 || c->wta_threads < 32 || c->wta_threads > 256 ||
@@ -1063,6 +1065,7 @@ DS_API int ds_set_kernel_config(ds_handle* h, const ds_kernel_config* c) {
         return h->fail(DS_INVALID_ARGUMENT, "block shape or prefetch depth out of range");
     if (c->fused_pairs) {
         if (h->ndirs != 4) return h->fail(DS_INVALID_ARGUMENT, "fused pairs need 4 paths");
+        if (c->lanes_per_line == 8) return h->fail(DS_INVALID_ARGUMENT, "fused pairs need 16 or 32 lanes per line");
         if (c->path_warps_per_block > 4 || c->horz_warps_per_block < 1 || c->horz_warps_per_block > 4)
             return h->fail(DS_INVALID_ARGUMENT, "fused pairs: 1..4 warps per direction per block");
         ds::KernelCfg t;

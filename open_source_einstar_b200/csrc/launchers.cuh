@@ -102,6 +102,10 @@ cudaError_t horz_seg(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedA
     namespace ds {                                                                                                   \
     cudaError_t launch_paths_r##R(const KernelCfg& cfg, bool c64, bool wide, const dsk::PathArgs& a, int ndirs,      \
                                   int max_lines, cudaStream_t st) {                                                  \
+        if (cfg.seg == 8) {                                                                                          \
+            if constexpr (R == 4 || R == 6 || R == 8) return paths_seg<R, 8>(cfg, c64, wide, a, ndirs, max_lines, st); \
+            return cudaErrorInvalidValue;                                                                            \
+        }                                                                                                            \
         DS_SEG_SWITCH(R, (paths_seg<R, (R <= 4 ? 16 : 32)>(cfg, c64, wide, a, ndirs, max_lines, st)),               \
                       (paths_seg<R, 32>(cfg, c64, wide, a, ndirs, max_lines, st)))                                   \
     }                                                                                                                \
@@ -237,6 +241,10 @@ cudaError_t bcosts_t(const dsk::CostArgs* args, const BatchGroupDev& g, cudaStre
     namespace ds {                                                                                                   \
     cudaError_t launch_paths_batch_r##R(const KernelCfg& cfg, bool c64, bool wide, const dsk::PathArgs* args,        \
                                         const BatchGroupDev& g, cudaStream_t st) {                                   \
+        if (cfg.seg == 8) {                                                                                          \
+            if constexpr (R == 4 || R == 6 || R == 8) return bpaths_seg<R, 8>(cfg, c64, wide, args, g, st);          \
+            return cudaErrorInvalidValue;                                                                            \
+        }                                                                                                            \
         DS_SEG_SWITCH(R, (bpaths_seg<R, (R <= 4 ? 16 : 32)>(cfg, c64, wide, args, g, st)),                           \
                       (bpaths_seg<R, 32>(cfg, c64, wide, args, g, st)))                                              \
     }                                                                                                                \

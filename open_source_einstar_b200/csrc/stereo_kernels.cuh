@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(256) k_cost_tiles(CostArgs a) {
 // ------------------------------------------------------------------------------------------------
 // Path aggregation (stereo.cpp:44-89, directions and start pixels :382-409).
 //
-// A segment of SEG lanes (16 or 32) runs one scanline; each lane holds NV = 2R consecutive
+// A segment of SEG lanes (8, 16 or 32) runs one scanline; each lane holds NV = 2R consecutive
 // disparities as R registers of two 16-bit lanes (k = sl*NV + 2r, +1). Per step and register:
 //   k-1 / k+1 neighbours   byte-permutes of adjacent registers (across lanes: one shuffle up, one down)
 //   k-2 / k+2 neighbours   the adjacent registers themselves (slant steps)
@@ -244,6 +244,7 @@ __device__ __forceinline__ void paths_body(const PathArgs& a, const int* p2, int
     const int len = live ? line_length(dx, dy, x0, y0, a.w, a.h) : 0;
     int nsteps = len;
     if constexpr (LPW == 2) nsteps = max(nsteps, __shfl_xor_sync(kFull, len, 16));
+    if constexpr (LPW == 4) nsteps = static_cast<int>(__reduce_max_sync(kFull, static_cast<unsigned>(len)));
 
     const CW* __restrict__ cl = static_cast<const CW*>(a.census_l);
     const CW* __restrict__ cr = static_cast<const CW*>(a.census_r);
