@@ -73,25 +73,46 @@ struct CensusArgs {
     int w, h, rx, ry, pitch;
 };
 
+// One 32 x 8 block of pixels per (bx, by): the block's image tile with its window halo is staged in
+// shared memory, then each thread builds its pixel's word from the tile. Every thread of the block
+// takes part in the staging (the persistent batch kernel calls this once per virtual block).
+constexpr int kCensusMaxRx = 4, kCensusMaxRy = 3;  // windows up to 9 x 7 (64-bit words)
+
 template <typename W>
 __device__ __forceinline__ void census_body(const CensusArgs& a, int bx, int by, int bz) {
-    const int x = bx * blockDim.x + threadIdx.x;
-    const int y = by * blockDim.y + threadIdx.y;
-    const int side = bz;
+    __shared__ uint8_t tile[8 + 2 * kCensusMaxRy][32 + 2 * kCensusMaxRx];
+    const int x0 = bx * 32, y0 = by * 8;
+    const uint8_t* img = a.img[bz];
+    const int tw = 32 + 2 * a.rx, th = 8 + 2 * a.ry;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    __syncthreads();  // the previous virtual block's readers are done
+    for (int i = tid; i < tw * th; i += 256) {
+        const int ty = i / tw, tx = i - ty * tw;
+        const int gx = x0 - a.rx + tx, gy = y0 - a.ry + ty;
+        tile[ty][tx] = (gx >= 0 && gx < a.w && gy >= 0 && gy < a.h) ? __ldg(img + static_cast<size_t>(gy) * a.w + gx) : 0;
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
     if (x >= a.w || y >= a.h) return;
-    const uint8_t* img = a.img[side];
     W word = 0;
     if (y >= a.ry && y < a.h - a.ry && x >= a.rx && x < a.w - a.rx) {
-        const uint8_t c = __ldg(img + static_cast<size_t>(y) * a.w + x);
-        for (int v = -a.ry; v <= a.ry; ++v) {
-            const uint8_t* row = img + static_cast<size_t>(y + v) * a.w + x;
-            for (int u = -a.rx; u <= a.rx; ++u) {
-                if (u == 0 && v == 0) continue;
-                word = static_cast<W>((word << 1) | static_cast<W>(__ldg(row + u) < c));
-            }
+        const int cx = threadIdx.x + a.rx, cy = threadIdx.y + a.ry;
+        const uint8_t c = tile[cy][cx];
+        if (a.rx == 2 && a.ry == 2) {  // the reference's default 5 x 5 window, unrolled
+#pragma unroll
+            for (int v = -2; v <= 2; ++v)
+#pragma unroll
+                for (int u = -2; u <= 2; ++u)
+                    if (u != 0 || v != 0) word = static_cast<W>((word << 1) | static_cast<W>(tile[cy + v][cx + u] < c));
+        } else {
+            for (int v = -a.ry; v <= a.ry; ++v)
+                for (int u = -a.rx; u <= a.rx; ++u) {
+                    if (u == 0 && v == 0) continue;
+                    word = static_cast<W>((word << 1) | static_cast<W>(tile[cy + v][cx + u] < c));
+                }
         }
     }
-    static_cast<W*>(a.out[side])[static_cast<size_t>(y) * a.pitch + x] = word;
+    static_cast<W*>(a.out[bz])[static_cast<size_t>(y) * a.pitch + x] = word;
 }
 
 template <typename W>
