@@ -404,7 +404,7 @@ void enqueue_frame(ds_handle* h, const uint8_t* left, const uint8_t* right, bool
         r.out_w = h->w;
         r.out_h = h->h;
         r.half = h->map_w == 2 * h->w ? 1 : 0;
-        dim3 b(32, 8), g((h->w + 31) / 32, (h->h + 7) / 8, 2);
+        dim3 b(32, 8), g((h->w + 32 * dsk::kRectifyPixelsPerThread - 1) / (32 * dsk::kRectifyPixelsPerThread), (h->h + 7) / 8, 2);
         dsk::k_rectify<<<g, b, 0, st>>>(r);
         ++g_launches;
         img[0] = h->d_rect[0];
@@ -1414,7 +1414,8 @@ void batch_plan_micro(ds_batch* b, ds_batch::Micro& m, const std::vector<int>& o
     for (int i : order) {
         ds_handle* h = b->h[i];
         const int tx = (h->w + 31) / 32, ty = (h->h + 7) / 8;
-        if (b->desc[i].raw) add(m.g_rect, i, tx * ty * 2, tx, ty);
+        const int tx4 = (h->w + 32 * dsk::kRectifyPixelsPerThread - 1) / (32 * dsk::kRectifyPixelsPerThread);
+        if (b->desc[i].raw) add(m.g_rect, i, tx4 * ty * 2, tx4, ty);
         add(m.g_post, i, tx * ty, tx, ty);
         {
             BatchGroup& g = find_or_add(m.g_census, [&](const BatchGroup& x) { return x.c64 == h->census64; });

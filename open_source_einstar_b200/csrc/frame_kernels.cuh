@@ -37,28 +37,51 @@ __device__ __forceinline__ uint32_t remap_sample(const uint8_t* __restrict__ src
     return static_cast<uint32_t>(__float2uint_rz(v));
 }
 
+// Four horizontally adjacent output pixels per thread (a block covers 128 x 8): the map entries come as
+// one 128-bit load per table and the four bytes leave as one 32-bit store when rows are 4-aligned.
+constexpr int kRectifyPixelsPerThread = 4;
+
 __device__ __forceinline__ void rectify_body(const RectifyArgs& a, int bx, int by, int bz) {
-    const int x = bx * blockDim.x + threadIdx.x;
+    const int x4 = (bx * blockDim.x + threadIdx.x) * kRectifyPixelsPerThread;
     const int y = by * blockDim.y + threadIdx.y;
     const int side = bz;
-    if (x >= a.out_w || y >= a.out_h) return;
+    if (x4 >= a.out_w || y >= a.out_h) return;
     const uint8_t* src = a.raw[side];
     const float* mx = a.map_x[side];
     const float* my = a.map_y[side];
-    uint32_t v;
+    const bool full = x4 + 4 <= a.out_w;
+    uint32_t v[4] = {0u, 0u, 0u, 0u};
     if (!a.half) {
-        const size_t i = static_cast<size_t>(y) * a.map_w + x;
-        v = remap_sample(src, a.raw_w, a.raw_h, __ldg(mx + i), __ldg(my + i));
+        const size_t i = static_cast<size_t>(y) * a.map_w + x4;
+        if (full && (a.map_w & 3) == 0) {
+            const float4 fx = __ldg(reinterpret_cast<const float4*>(mx + i));
+            const float4 fy = __ldg(reinterpret_cast<const float4*>(my + i));
+            v[0] = remap_sample(src, a.raw_w, a.raw_h, fx.x, fy.x);
+            v[1] = remap_sample(src, a.raw_w, a.raw_h, fx.y, fy.y);
+            v[2] = remap_sample(src, a.raw_w, a.raw_h, fx.z, fy.z);
+            v[3] = remap_sample(src, a.raw_w, a.raw_h, fx.w, fy.w);
+        } else {
+            for (int j = 0; j < 4 && x4 + j < a.out_w; ++j)
+                v[j] = remap_sample(src, a.raw_w, a.raw_h, __ldg(mx + i + j), __ldg(my + i + j));
+        }
     } else {
-        uint32_t acc = 0;
-        for (int j = 0; j < 2; ++j)
-            for (int i = 0; i < 2; ++i) {
-                const size_t m = static_cast<size_t>(2 * y + j) * a.map_w + (2 * x + i);
-                acc += remap_sample(src, a.raw_w, a.raw_h, __ldg(mx + m), __ldg(my + m));
-            }
-        v = (acc + 2u) / 4u;
+        for (int j = 0; j < 4 && x4 + j < a.out_w; ++j) {
+            const int x = x4 + j;
+            uint32_t acc = 0;
+            for (int jj = 0; jj < 2; ++jj)
+                for (int ii = 0; ii < 2; ++ii) {
+                    const size_t m = static_cast<size_t>(2 * y + jj) * a.map_w + (2 * x + ii);
+                    acc += remap_sample(src, a.raw_w, a.raw_h, __ldg(mx + m), __ldg(my + m));
+                }
+            v[j] = (acc + 2u) / 4u;
+        }
     }
-    a.out[side][static_cast<size_t>(y) * a.out_w + x] = static_cast<uint8_t>(v);
+    uint8_t* out = a.out[side] + static_cast<size_t>(y) * a.out_w + x4;
+    if (full && (a.out_w & 3) == 0) {
+        *reinterpret_cast<uint32_t*>(out) = v[0] | (v[1] << 8) | (v[2] << 16) | (v[3] << 24);
+    } else {
+        for (int j = 0; j < 4 && x4 + j < a.out_w; ++j) out[j] = static_cast<uint8_t>(v[j]);
+    }
 }
 
 static __global__ void k_rectify(RectifyArgs a) { rectify_body(a, blockIdx.x, blockIdx.y, blockIdx.z); }
