@@ -247,6 +247,35 @@ DS_API int ds_batch_get_options(const ds_batch* batch, ds_batch_options* out);
 DS_API int ds_batch_profile(ds_batch* batch, int on);
 DS_API int ds_batch_stage_ms(ds_batch* batch, double* ms);
 
+/* ---- Points, normals, weights (the hand-off to tracking) and the recording layout of depth ----------------
+ * depth::PointImageParams (libs/depth/include/einstar/depth/point_image.hpp:41-47). */
+typedef struct ds_point_params {
+    float min_depth_mm;              /* 150 */
+    float max_depth_mm;              /* 700 */
+    float max_depth_jump_mm;         /* 4: neighbours used for normals */
+    float edge_weight;               /* 0.25: view term of a point without a normal */
+    float weight_reference_depth_mm; /* 0: no depth-noise term */
+} ds_point_params;
+DS_API void ds_default_point_params(ds_point_params* params);
+
+/* depth::disparity_to_points (libs/depth/src/point_image.cpp:10-54) on device buffers, enqueued on
+ * `stream` (a cudaStream_t; NULL = the default stream): organised points in the rectified left frame
+ * (float4 x, y, z, w = 1 where valid, 0 elsewhere), unit normals towards the camera (float4, w = 0; zero
+ * where unknown) and weights (confidence x view term x depth-noise term). `confidence` may be NULL
+ * (weight 1). points_xyzw and normals_xyzw hold width * height float4, 16-byte aligned. Allocates
+ * nothing. The Metal port's counterpart: disparity_points / point_normals
+ * (libs/depth_metal/src/stereo_kernels.metal.inc:719-766). */
+DS_API int ds_disparity_to_points(const float* disparity, const float* confidence, int width, int height,
+                                  const ds_geometry* geometry, const ds_point_params* params, float* points_xyzw,
+                                  float* normals_xyzw, float* weights, void* stream);
+
+/* depth_metal::DepthPacker::pack (libs/depth_metal/src/depth_packer.cpp:10-21): the session file's
+ * uncompressed depth layout, width * height * 3 bytes on the device: u16 depth in 1/50 mm delta-coded
+ * along each row (value minus its left neighbour's, mod 2^16; 0 = no depth), then u8 confidence
+ * round(weight * 255). `packed` must be 2-byte aligned. */
+DS_API int ds_pack_depth(const float* points_xyzw, const float* weights, int width, int height, uint8_t* packed,
+                         void* stream);
+
 /* ---- Request server: continuous batching of frames as they arrive (no counterpart in the reference,
  * whose frontend runs one camera pair synchronously, libs/pipeline/src/stereo_frontend.cpp:302-330) ------
  * A worker thread admits submitted frames in arrival order as soon as a slot (a CUDA stream with its own

@@ -18,3 +18,4 @@ from .stereo import (  # noqa: F401
     valid_disparity,
 )
 from .batch import PairDesc, StereoBatch  # noqa: F401,E402
+from .points import PointImageParams, disparity_to_points, pack_depth  # noqa: F401,E402

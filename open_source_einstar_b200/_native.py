@@ -59,6 +59,11 @@ class BatchOptionsC(C.Structure):
     _fields_ = [("micro_batch", C.c_int), ("branches", C.c_int)]
 
 
+class PointParamsC(C.Structure):
+    _fields_ = [("min_depth_mm", C.c_float), ("max_depth_mm", C.c_float), ("max_depth_jump_mm", C.c_float),
+                ("edge_weight", C.c_float), ("weight_reference_depth_mm", C.c_float)]
+
+
 class ServerOptionsC(C.Structure):
     _fields_ = [("volume_budget_bytes", C.c_size_t), ("max_slots", C.c_int), ("max_pending", C.c_int)]
 
@@ -115,6 +120,9 @@ SIGNATURES = {
     "ds_batch_get_options": (_i, [_vp, C.POINTER(BatchOptionsC)]),
     "ds_batch_profile": (_i, [_vp, _i]),
     "ds_batch_stage_ms": (_i, [_vp, _vp]),
+    "ds_default_point_params": (None, [C.POINTER(PointParamsC)]),
+    "ds_disparity_to_points": (_i, [_vp, _vp, _i, _i, C.POINTER(GeometryC), C.POINTER(PointParamsC), _vp, _vp, _vp, _vp]),
+    "ds_pack_depth": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
     "ds_server_create": (_i, [C.POINTER(ServerOptionsC), C.POINTER(_vp)]),
     "ds_server_destroy": (None, [_vp]),
     "ds_server_last_error": (C.c_char_p, [_vp]),

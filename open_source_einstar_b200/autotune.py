@@ -90,19 +90,32 @@ def stage_candidates(kind: FrameKind, stage: int, best: dict | None = None, fuse
     return [{**best, "wta_threads": t} for t in (128, 256)]
 
 
-def search(kind: FrameKind, time_fn, fused_ok: bool = True) -> tuple[dict, dict]:
-    """Staged search; time_fn(config) -> ms per frame (inf if the configuration is rejected).
+def search(kind: FrameKind, time_fn, fused_ok: bool = True, keep: int = 2) -> tuple[dict, dict]:
+    """Staged search; time_fn(config) -> ms per frame (inf if the configuration is rejected). The `keep`
+    fastest shapes of stage 1 each go through stage 2 (a shape's best block size can reorder them).
     Returns (best configuration, {stage: [(config, ms), ...]})."""
     log: dict = {}
     best, best_ms = None, float("inf")
-    for stage in (1, 2, 3):
-        trials = []
-        for cfg in stage_candidates(kind, stage, best, fused_ok):
+    trials = [(cfg, time_fn(cfg)) for cfg in stage_candidates(kind, 1, None, fused_ok)]
+    log[1] = trials
+    finite = sorted((t for t in trials if t[1] != float("inf")), key=lambda t: t[1])
+    if finite:
+        best, best_ms = finite[0]
+    seeds = [c for c, _ in finite[:keep]]
+    log[2] = []
+    for seed in seeds:
+        for cfg in stage_candidates(kind, 2, seed, fused_ok):
             ms = time_fn(cfg)
-            trials.append((cfg, ms))
+            log[2].append((cfg, ms))
             if ms < best_ms:
                 best, best_ms = cfg, ms
-        log[stage] = trials
+    log[3] = []
+    if best is not None:
+        for cfg in stage_candidates(kind, 3, best, fused_ok):
+            ms = time_fn(cfg)
+            log[3].append((cfg, ms))
+            if ms < best_ms:
+                best, best_ms = cfg, ms
     return best, {"ms": best_ms, "trials": log}
 
 
@@ -149,7 +162,7 @@ class Autotuner:
             hit = self.lookup(kind, dev, fused_ok)
             if hit:
                 return hit
-        time_fn = device_timer(kind, frames, warmup, params)
+        time_fn = device_timer(kind, frames, warmup, params) if fused_ok else batch_timer(kind, warmup, params)
         best, info = search(kind, time_fn, fused_ok)
         self.table[self._key(kind, dev, fused_ok)] = {
             "config": best, "ms_per_frame": info["ms"],
@@ -218,6 +231,50 @@ def device_timer(kind: FrameKind, frames: int, warmup: int, params=None):
         rows = s.profile_collect()
         s.profile(False)
         return float(np.median(rows.sum(axis=1))) if len(rows) else float("inf")
+
+    return time_fn
+
+
+def batch_timer(kind: FrameKind, warmup: int, params=None, pairs: int = 8, reps: int = 3):
+    """time_fn for the batched path: a StereoBatch of `pairs` frames of this kind with the library's default
+    schedule; device time of one graph replay per frame, best of `reps`."""
+    import torch
+
+    from .batch import PairDesc, StereoBatch
+    from .stereo import SgmParams, StereoError, StereoParams
+    from .synth import plane_sphere_pair
+    dev = torch.device("cuda")
+    pr = plane_sphere_pair(seed=7, width=kind.width, height=kind.height, f=1.4 * kind.width,
+                           num_disparities=kind.num_disparities, device=dev)
+    if params is None:
+        params = StereoParams(sgm=SgmParams(min_disparity=pr.min_disparity, num_disparities=kind.num_disparities,
+                                            eight_paths=kind.eight_paths), wide_costs=kind.wide)
+    l = torch.from_numpy(pr.left).to(dev)
+    r = torch.from_numpy(pr.right).to(dev)
+    outs = [{"disparity_u16": torch.empty((kind.height, kind.width), dtype=torch.int16, device=dev)} for _ in range(pairs)]
+    st = torch.cuda.Stream(dev)
+
+    def time_fn(cfg: dict) -> float:
+        try:
+            b = StereoBatch([PairDesc(kind.width, kind.height, params, kernel=cfg)] * pairs, tuned=False)
+        except StereoError:
+            return float("inf")
+        try:
+            for i, o in enumerate(outs):
+                b.bind(i, l, r, o)
+            for _ in range(max(warmup, 1)):
+                b.run(stream=st)
+            best = float("inf")
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                b.run(stream=st)
+                e1.record(st)
+                e1.synchronize()
+                best = min(best, e0.elapsed_time(e1) / pairs)
+            return best
+        finally:
+            b.close()
 
     return time_fn
 

@@ -95,6 +95,8 @@ class Port:
         L.orc_remap.argtypes = [vp, i, i, vp, vp, i, i, vp]
         L.orc_depth.argtypes = [vp, i, i, d, d, d, f, f, vp]
         L.orc_encode_u16.argtypes = [vp, C.c_long, i, vp]
+        L.orc_points.argtypes = [vp, vp, i, i, d, d, d, d, d, f, f, f, f, f, vp, vp, vp]
+        L.orc_pack_depth.argtypes = [vp, vp, i, i, vp]
 
     def census(self, img, rx=2, ry=2) -> np.ndarray:
         img = _u8(img)
@@ -157,6 +159,29 @@ class Port:
         h, w = d.shape
         out = np.empty_like(d)
         self.lib.orc_depth(_p(d), w, h, float(f), float(baseline), float(cx_offset), float(min_depth), float(max_depth), _p(out))
+        return out
+
+    def points(self, disp, conf, f, cx, cy, baseline, cx_offset=0.0, min_depth=150.0, max_depth=700.0,
+               max_jump=4.0, edge_weight=0.25, weight_reference_depth=0.0):
+        """depth::disparity_to_points restated (point_image.cpp:10-54): (points xyzw, normals xyzw, weights)."""
+        dd = np.ascontiguousarray(disp, np.float32)
+        h, w = dd.shape
+        cf = None if conf is None else np.ascontiguousarray(conf, np.float32)
+        pts = np.empty((h, w, 4), np.float32)
+        nrm = np.empty((h, w, 4), np.float32)
+        wts = np.empty((h, w), np.float32)
+        self.lib.orc_points(_p(dd), None if cf is None else _p(cf), w, h, float(f), float(cx), float(cy), float(baseline),
+                            float(cx_offset), float(min_depth), float(max_depth), float(max_jump), float(edge_weight),
+                            float(weight_reference_depth), _p(pts), _p(nrm), _p(wts))
+        return pts, nrm, wts
+
+    def pack_depth(self, points_xyzw, weights) -> np.ndarray:
+        """depth_metal::DepthPacker restated (depth_packer.cpp:10-21): w*h*3 bytes."""
+        p = np.ascontiguousarray(points_xyzw, np.float32)
+        wt = np.ascontiguousarray(weights, np.float32)
+        h, w = wt.shape
+        out = np.empty(h * w * 3, np.uint8)
+        self.lib.orc_pack_depth(_p(p), _p(wt), w, h, _p(out))
         return out
 
     def encode_u16(self, disp, min_disparity) -> np.ndarray:

@@ -308,3 +308,98 @@ void orc_encode_u16(const float* disp, long n, int min_disparity, uint16_t* out)
         out[i] = (uint16_t)v;
     }
 }
+
+/* Vec3f arithmetic as Eigen evaluates it for 3 floats (no fused multiply-add: built with
+ * -ffp-contract=off): dot = (x*x' + y*y') + z*z', cross component-wise, norm = sqrt(dot(v, v)). */
+static float dot3(const float* a, const float* b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; }
+
+void orc_points(const float* disp, const float* conf, int w, int h, double f, double cx, double cy, double baseline,
+                double cx_offset, float min_depth, float max_depth, float max_jump, float edge_weight,
+                float weight_reference_depth, float* points, float* normals, float* weights) {
+    const size_t n = (size_t)w * (size_t)h;
+    for (size_t i = 0; i < n; ++i) {
+        for (int c = 0; c < 4; ++c) points[4 * i + c] = normals[4 * i + c] = 0.0f;
+        weights[i] = 0.0f;
+    }
+    /* point_image.cpp:15-25 */
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            const size_t i = (size_t)y * w + x;
+            const float d = disp[i];
+            if (!(d > -1.0e8f) || (double)d + cx_offset <= 0.0) continue;
+            const double z = f * baseline / ((double)d + cx_offset);
+            if (z < (double)min_depth || z > (double)max_depth) continue;
+            points[4 * i + 0] = (float)(((double)x - cx) * z / f);
+            points[4 * i + 1] = (float)(((double)y - cy) * z / f);
+            points[4 * i + 2] = (float)z;
+            points[4 * i + 3] = 1.0f;
+            weights[i] = conf ? conf[i] : 1.0f;
+        }
+    /* point_image.cpp:27-51 */
+    const float rc[3] = {(float)baseline, 0.0f, 0.0f};
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            const size_t i = (size_t)y * w + x;
+            const float* p = points + 4 * i;
+            if (p[2] == 0.0f) continue;
+            float view = edge_weight;
+            if (x > 0 && y > 0 && x + 1 < w && y + 1 < h) {
+                const float* l = points + 4 * (i - 1);
+                const float* r = points + 4 * (i + 1);
+                const float* u = points + 4 * (i - (size_t)w);
+                const float* dn = points + 4 * (i + (size_t)w);
+                if (l[2] != 0 && r[2] != 0 && u[2] != 0 && dn[2] != 0 && fabsf(l[2] - r[2]) <= max_jump &&
+                    fabsf(u[2] - dn[2]) <= max_jump) {
+                    const float a[3] = {r[0] - l[0], r[1] - l[1], r[2] - l[2]};
+                    const float b[3] = {dn[0] - u[0], dn[1] - u[1], dn[2] - u[2]};
+                    float nn[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+                    const float len = sqrtf(dot3(nn, nn));
+                    if (len >= 1e-9f) {
+                        for (int c = 0; c < 3; ++c) nn[c] = nn[c] / len;
+                        if (dot3(nn, p) > 0) for (int c = 0; c < 3; ++c) nn[c] = -nn[c];
+                        for (int c = 0; c < 3; ++c) normals[4 * i + c] = nn[c];
+                        const float pl = sqrtf(dot3(p, p));
+                        const float pn[3] = {p[0] / pl, p[1] / pl, p[2] / pl};
+                        const float q[3] = {p[0] - rc[0], p[1] - rc[1], p[2] - rc[2]};
+                        const float ql = sqrtf(dot3(q, q));
+                        const float qn[3] = {q[0] / ql, q[1] / ql, q[2] / ql};
+                        const float v1 = -dot3(nn, pn), v2 = -dot3(nn, qn);
+                        const float m = v1 < v2 ? v1 : v2;
+                        view = 0.0f > m ? 0.0f : m;
+                    }
+                }
+            }
+            float dw = 1.0f; /* depth_noise_weight, point_image.hpp:56-60 */
+            if (weight_reference_depth > 0.0f) {
+                const float rr = weight_reference_depth / p[2];
+                const float r2 = rr * rr;
+                dw = r2 > 1.0f ? 1.0f : (r2 < 0.1f ? 0.1f : r2);
+            }
+            weights[i] *= view * dw;
+        }
+}
+
+static uint32_t quantize_mm50(float z) {
+    if (!(z > 0.0f)) return 0u;
+    float q = roundf(z * 50.0f);
+    if (q < 1.0f) q = 1.0f;
+    if (q > 65535.0f) q = 65535.0f;
+    return (uint32_t)q;
+}
+
+void orc_pack_depth(const float* points_xyzw, const float* weights, int w, int h, uint8_t* out) {
+    const size_t n = (size_t)w * (size_t)h;
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            const size_t i = (size_t)y * w + x;
+            const uint32_t q = quantize_mm50(points_xyzw[4 * i + 2]);
+            const uint32_t left = x > 0 ? quantize_mm50(points_xyzw[4 * (i - 1) + 2]) : 0u;
+            const uint16_t dq = (uint16_t)((q - left) & 0xFFFFu);
+            out[2 * i] = (uint8_t)(dq & 0xFF);
+            out[2 * i + 1] = (uint8_t)(dq >> 8);
+            float c = roundf(weights[i] * 255.0f);
+            if (c < 0.0f) c = 0.0f;
+            if (c > 255.0f) c = 255.0f;
+            out[2 * n + i] = (uint8_t)c;
+        }
+}

@@ -49,6 +49,18 @@ void orc_depth(const float* disp, int w, int h, double f, double baseline, doubl
                float* depth);
 void orc_encode_u16(const float* disp, long n, int min_disparity, uint16_t* out);
 
+/* depth::disparity_to_points (libs/depth/src/point_image.cpp:10-54; params point_image.hpp:41-54):
+ * organised points in the rectified left frame (xyzw, w = 1 where valid), unit normals towards the camera
+ * (xyzw, w = 0) from central differences, and weights = confidence x view term x depth-noise term.
+ * `conf` may be NULL (weight 1). */
+void orc_points(const float* disp, const float* conf, int w, int h, double f, double cx, double cy, double baseline,
+                double cx_offset, float min_depth, float max_depth, float max_jump, float edge_weight,
+                float weight_reference_depth, float* points, float* normals, float* weights);
+
+/* depth_metal::DepthPacker (libs/depth_metal/src/depth_packer.cpp:10-21): u16 depth in 1/50 mm,
+ * delta-coded along rows (q - q_left, mod 2^16), then u8 confidence round(w * 255); out = w*h*3 bytes. */
+void orc_pack_depth(const float* points_xyzw, const float* weights, int w, int h, uint8_t* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,7 +35,7 @@ def test_staged_search_finds_the_fastest_of_each_stage():
                     "wta_threads": 128, "prefetch_steps": 8, "fused_pairs": 0, "horz_warps_per_block": 4}
     assert info["ms"] == pytest.approx(1.0)
     n = sum(len(v) for v in info["trials"].values())
-    assert n <= 20  # staged, not the full product
+    assert n <= 30  # staged: two shapes go through the block search, not the full product (~100)
 
 
 def test_rejected_configurations_are_skipped():
