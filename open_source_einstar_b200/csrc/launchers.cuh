@@ -203,7 +203,9 @@ template <int R, int SEG, typename CW, typename ST, bool MAT>
 cudaError_t bpaths_t(const KernelCfg& cfg, const dsk::PathArgs* args, const BatchGroupDev& g, cudaStream_t st) {
     auto k = cfg.prefetch == 8 ? dsk::kb_paths<R, SEG, CW, ST, MAT, 8> : dsk::kb_paths<R, SEG, CW, ST, MAT, 4>;
     const int threads = cfg.paths_warps * 32;
-    k<<<persistent_grid(k, threads, 0, g.total), threads, 0, st>>>(args, g.pairs, g.prefix, g.gx, g.n, g.total);
+    // One block per virtual block: scanline groups of different pairs differ in length, and the block
+    // scheduler balances them better than a fixed share per resident block.
+    k<<<g.total, threads, 0, st>>>(args, g.pairs, g.prefix, g.gx, g.n, g.total);
     return cudaGetLastError();
 }
 
@@ -224,7 +226,8 @@ cudaError_t bwta_t(const KernelCfg& cfg, int ndirs, const dsk::WtaArgs* args, co
         const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return e;
     }
-    k<<<persistent_grid(k, cfg.wta_threads, smem, g.total), cfg.wta_threads, smem, st>>>(args, g.pairs, g.prefix, g.gx, g.n, g.total);
+    // One block per row: rows are few (about 2-3 per resident block), so a fixed share leaves a tail.
+    k<<<g.total, cfg.wta_threads, smem, st>>>(args, g.pairs, g.prefix, g.gx, g.n, g.total);
     return cudaGetLastError();
 }
 
