@@ -378,8 +378,8 @@ __global__ void __launch_bounds__(256) k_paths(PathArgs a) {
 // reference's u16 sums, wrap included); left WTA = segment min of (cost << 16 | k) keys (first strict
 // minimum), best non-adjacent cost by a second reduction, uniqueness as a float compare, parabola from
 // the neighbours' costs. Right WTA: every candidate (x, k) offers its key to right pixel x - min - k by
-// a shared-memory atomicMin, which leaves the first strict minimum along that diagonal. Candidates are
-// selected by all-ones masks OR-ed into keys and sums, so there are no per-element branches.
+// a shared-memory atomicMin, which leaves the first strict minimum along that diagonal. Warps whose
+// pixels are interior (every disparity has a right column) skip the per-element range tests.
 
 struct WtaArgs {
     const void* values;
@@ -431,14 +431,15 @@ __device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
     const int per_warp = 32 / SEG;
     const int stride = nwarps * per_warp;
     // Per register r: the (k, k + 1) index pair of the keys, and masks of the disparities >= nd (padding
-    // of the lane slabs).
-    uint32_t kk[R], pada[R], padb[R];
+    // of the lane slabs): full keys and 16-bit halves.
+    uint32_t kk[R], pada[R], padb[R], padh[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int ka = k0 + 2 * r;
         kk[r] = static_cast<uint32_t>(ka) | (static_cast<uint32_t>(ka + 1) << 16);
         pada[r] = ka >= a.nd ? kEmpty : 0u;
         padb[r] = ka + 1 >= a.nd ? kEmpty : 0u;
+        padh[r] = (pada[r] & 0xFFFFu) | (padb[r] & 0xFFFF0000u);
     }
     // Double buffer: the next pixel's chunks are in flight while this one is reduced.
     uint32_t nxt[NDIRS][VW];
@@ -484,33 +485,20 @@ __device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
         const int lo = max(0, xc - a.min_disp - (a.w - 1));
         const int hi = min(a.nd, xc - a.min_disp + 1);
         const int rbase = xc - a.min_disp - k0;  // right column of the lane's first disparity
-        // Candidate masks (all ones where disparity k is not a candidate of this pixel: outside [lo, hi)
-        // or padding). Interior warps (every k < nd has a right column) take the padding masks as they are.
-        uint32_t ma[R], mb[R];
+        uint32_t key, second;
         if (__all_sync(kFull, live && lo == 0 && hi == a.nd)) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) ma[r] = pada[r], mb[r] = padb[r];
-        } else {
-            const unsigned span = live ? static_cast<unsigned>(max(hi - lo, 0)) : 0u;
-            const int base = k0 - lo;
+            // Interior pixels (every disparity < nd matches a column of the right row): no per-element
+            // range tests; padding keys are all ones and take part in nothing.
+            uint32_t kmin = kEmpty;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                ma[r] = static_cast<unsigned>(base + 2 * r) < span ? 0u : kEmpty;
-                mb[r] = static_cast<unsigned>(base + 2 * r + 1) < span ? 0u : kEmpty;
+                const uint32_t key_a = prmt(kk[r], tot[r], 0x5410) | pada[r];  // (cost_a << 16) | ka
+                const uint32_t key_b = prmt(kk[r], tot[r], 0x7632) | padb[r];  // (cost_b << 16) | ka + 1
+                kmin = min(kmin, min(key_a, key_b));
+                if (key_a != kEmpty) atomicMin(&rkey[rbase - 2 * r], key_a);
+                if (key_b != kEmpty) atomicMin(&rkey[rbase - 2 * r - 1], key_b);
             }
-        }
-        uint32_t kmin = kEmpty;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const uint32_t key_a = prmt(kk[r], tot[r], 0x5410) | ma[r];  // (cost_a << 16) | ka
-            const uint32_t key_b = prmt(kk[r], tot[r], 0x7632) | mb[r];  // (cost_b << 16) | ka + 1
-            kmin = min(kmin, min(key_a, key_b));
-            if (key_a != kEmpty) atomicMin(&rkey[rbase - 2 * r], key_a);
-            if (key_b != kEmpty) atomicMin(&rkey[rbase - 2 * r - 1], key_b);
-        }
-        const uint32_t key = seg_min<SEG>(kmin, seg);
-        uint32_t second;
-        {
+            key = seg_min<SEG>(kmin, seg);
             const int bk = static_cast<int>(key & 0xFFFFu);
             uint32_t m2 = kEmpty;
 #pragma unroll
@@ -519,9 +507,35 @@ __device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
                 // disparities within one of bk are not the second minimum (stereo.cpp:420-424)
                 const uint32_t ex = (static_cast<unsigned>(ka - bk + 1) <= 2u ? 0x0000FFFFu : 0u) |
                                     (static_cast<unsigned>(ka - bk + 2) <= 2u ? 0xFFFF0000u : 0u);
-                m2 = vmin2(m2, tot[r] | (ma[r] & 0x0000FFFFu) | (mb[r] & 0xFFFF0000u) | ex);
+                m2 = vmin2(m2, tot[r] | padh[r] | ex);
             }
             second = seg_min<SEG>(hmin2(m2), seg);
+        } else {
+            uint32_t kmin = kEmpty;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int ka = k0 + 2 * r;
+                const uint32_t key_a = prmt(kk[r], tot[r], 0x5410);
+                const uint32_t key_b = prmt(kk[r], tot[r], 0x7632);
+                if (live && ka >= lo && ka < hi) {
+                    kmin = min(kmin, key_a);
+                    atomicMin(&rkey[rbase - 2 * r], key_a);
+                }
+                if (live && ka + 1 >= lo && ka + 1 < hi) {
+                    kmin = min(kmin, key_b);
+                    atomicMin(&rkey[rbase - 2 * r - 1], key_b);
+                }
+            }
+            key = seg_min<SEG>(kmin, seg);
+            const int bk = static_cast<int>(key & 0xFFFFu);
+            uint32_t sec = 0xFFFFu;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int ka = k0 + 2 * r;
+                if (ka >= lo && ka < hi && (ka - bk > 1 || bk - ka > 1)) sec = min(sec, tot[r] & 0xFFFFu);
+                if (ka + 1 >= lo && ka + 1 < hi && (ka + 1 - bk > 1 || bk - ka - 1 > 1)) sec = min(sec, tot[r] >> 16);
+            }
+            second = seg_min<SEG>(sec, seg);
         }
         const int bk = static_cast<int>(key & 0xFFFFu);
         const int km = max(bk - 1, 0), kp = min(bk + 1, a.nd - 1);
