@@ -2,10 +2,10 @@
 
 The reference re-runs depth on recorded raw IR pairs one frame at a time through its frontend. OfflineRedepth
 runs them in batches of `batch_size` pairs instead, each batch one StereoBatch graph replay. Two batches
-alternate: while one runs, the raw pairs of the next are copied to the device on a second stream, and
-the results of the previous one are copied back. All frames share one calibration (resident remap
-tables) and one parameter set. That is typically 8-path SGM with 16-bit path values at D=256 for
-offline quality.
+alternate over three streams: while one runs, the raw pairs of the next are copied to the device and
+the results of the previous one are copied back, on the GPU's separate copy engines. All frames share
+one calibration (resident remap tables) and one parameter set. That is typically 8-path SGM with
+16-bit path values at D=256 for offline quality.
 """
 from __future__ import annotations
 
@@ -39,7 +39,8 @@ class OfflineRedepth:
         dev = torch.device("cuda")
         self.dev = dev
         self.compute = torch.cuda.Stream(dev)
-        self.copy = torch.cuda.Stream(dev)
+        self.copy = torch.cuda.Stream(dev)       # host -> device
+        self.copy_out = torch.cuda.Stream(dev)   # device -> host
         desc = PairDesc(self.w, self.h, params, raw=True, calib=0, geometry=geometry, kernel=kernel,
                         min_depth=depth_range[0], max_depth=depth_range[1])
         self.batches, self.inputs, self.outputs = [], [], []
@@ -58,6 +59,7 @@ class OfflineRedepth:
             self.outputs.append(outs)
         self.h2d_done = [torch.cuda.Event(), torch.cuda.Event()]
         self.run_done = [torch.cuda.Event(), torch.cuda.Event()]
+        self.d2h_done = [torch.cuda.Event(), torch.cuda.Event()]
 
     def close(self):
         for b in self.batches:
@@ -99,7 +101,8 @@ class OfflineRedepth:
 
         def download(k):
             s = k % 2
-            with torch.cuda.stream(self.compute):
+            with torch.cuda.stream(self.copy_out):
+                self.copy_out.wait_event(self.run_done[s])
                 for j in range(self.n):
                     i = k * self.n + j
                     if i >= N:
@@ -108,16 +111,22 @@ class OfflineRedepth:
                     torch.from_numpy(out_u16[i].view(np.int16)).copy_(o["disparity_u16"], non_blocking=True)
                     if out_depth is not None and "depth" in o:
                         torch.from_numpy(out_depth[i]).copy_(o["depth"], non_blocking=True)
+                self.d2h_done[s].record(self.copy_out)
 
+        # Three streams: inputs in, graph replays, results out. A buffer set is reused two batches later,
+        # after its results have left (d2h_done) and its inputs were consumed (run_done).
         upload(0)
         for k in range(nb):
             s = k % 2
             if k + 1 < nb:
                 upload(k + 1)
             self.compute.wait_event(self.h2d_done[s])
+            self.compute.wait_event(self.d2h_done[s])
             self.batches[s].run(stream=self.compute)
-            download(k)
             self.run_done[s].record(self.compute)
+            download(k)
+        for s in range(min(nb, 2)):
+            self.compute.wait_event(self.d2h_done[s])
         end.record(self.compute)
         end.synchronize()
         return OfflineStats(N, nb, start.elapsed_time(end), self.device_bytes)
