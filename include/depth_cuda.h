@@ -61,20 +61,38 @@ typedef struct ds_sgm_params {
     int lr_max_diff;
 } ds_sgm_params;
 
-/* depth::StereoParams (stereo.hpp:80-88) reduced to the hot path. The stages after SGM that this
- * library does not run (pyramid + ZNCC refinement, detail refinement, occlusion / spike filters,
- * speckle removal) keep their switches so that a caller asking for them gets DS_UNSUPPORTED instead
- * of silently different results. */
+/* depth::StereoParams (libs/depth/include/einstar/depth/stereo.hpp:41-88). With pyramid_levels = 0 and
+ * the later stages off (ds_default_params) a frame is the hot path: SGM, L-R check and, with `median`,
+ * a 3x3 median. Any of pyramid_levels > 0, detail_enabled, filter_occlusion, filter_spikes or
+ * speckle_max_region_size > 1 selects depth::compute_disparity (stereo.cpp:501-536) instead: SGM at the
+ * pyramid's coarsest level, slanted-window ZNCC refinement up to the stereo resolution, detail refinement
+ * on the full-resolution pair (ds_compute_raw with remap tables at twice the stereo size), occlusion and
+ * spike filters, speckle removal; the confidence is then the ZNCC score and `median` is not applied.
+ * Those frames run through ds_compute* only (not in batches or the request server). */
 typedef struct ds_stereo_params {
-    int pyramid_levels;          /* must be 0 */
+    int pyramid_levels;          /* 0..4: SGM at 1/2^levels of the stereo resolution */
     ds_sgm_params sgm;
-    int subpixel;                /* parabola fit in the WTA (stereo.cpp:430-431) */
-    int median;                  /* 3x3 median of valid neighbours after the L-R check (stereo.cpp:129-147) */
-    int detail_enabled;          /* must be 0 */
-    int filter_occlusion;        /* must be 0 */
-    int filter_spikes;           /* must be 0 */
-    int speckle_max_region_size; /* must be 0 */
+    int subpixel;                /* parabola fit in the WTA (stereo.cpp:430-431) and the refinements */
+    int median;                  /* hot path: 3x3 median of valid neighbours after the L-R check (stereo.cpp:129-147) */
+    int detail_enabled;          /* depth::DetailParams::enabled */
+    int filter_occlusion;        /* depth::FilterParams::occlusion */
+    int filter_spikes;           /* depth::FilterParams::spikes */
+    int speckle_max_region_size; /* depth::SpeckleParams::max_region_size (reference default 200) */
     int wide_costs;              /* 1: 16-bit path values even when census window + P2 <= 255 */
+    /* depth::RefineParams (stereo.hpp:41-47) */
+    int refine_search_radius;    /* 2 */
+    int refine_zncc_radius;      /* 3 (7 x 7 window) */
+    float refine_min_zncc;       /* 0.5 */
+    int refine_reject_edge_winners; /* 1 */
+    /* depth::DetailParams (stereo.hpp:53-61) */
+    int detail_radius;           /* 5 (10 x 10 full-resolution window) */
+    float detail_search;         /* 1 */
+    float detail_step;           /* 0.5 */
+    float detail_min_zncc;       /* 0.5 */
+    /* depth::FilterParams, depth::SpeckleParams (stereo.hpp:66-79) */
+    float occlusion_tolerance;   /* 1 */
+    float spike_threshold;       /* 1 */
+    float speckle_max_diff;      /* 1 */
 } ds_stereo_params;
 
 /* depth::RectifiedGeometry (libs/depth/include/einstar/depth/point_image.hpp:12-26). */
@@ -105,7 +123,8 @@ typedef struct ds_outputs {
 
 typedef struct ds_handle ds_handle;
 
-/* Hot-path defaults: depth::SgmParams defaults, pyramid 0, subpixel and median on, other stages off. */
+/* Hot-path defaults: depth::SgmParams defaults, pyramid 0, subpixel and median on, the later stages off
+ * (their parameters at the reference's defaults). */
 DS_API void ds_default_params(ds_stereo_params* params);
 
 /* MetalStereo::create (metal_stereo.hpp:70-71; validation as metal_stereo.cpp:115-120). */

@@ -56,7 +56,24 @@ struct SgmParams {
     int lr_max_diff = 1;
 };
 
-// depth::StereoParams reduced to the hot path (the other stages answer Errc::unsupported).
+// depth::RefineParams, depth::DetailParams (libs/depth/include/einstar/depth/stereo.hpp:42-63).
+struct RefineParams {
+    int search_radius = 2;
+    int zncc_radius = 3;
+    float min_zncc = 0.5f;
+    bool reject_edge_winners = true;
+};
+
+struct DetailParams {
+    int radius = 5;
+    float search = 1.0f;
+    float step = 0.5f;
+    float min_zncc = 0.5f;
+};
+
+// depth::StereoParams with this library's defaults: the hot path (pyramid 0, the later stages off).
+// pyramid_levels > 0, detail_enabled, the filters or speckle_max_region_size > 1 run the whole of
+// depth::compute_disparity (refinement, detail, filters, speckles; see ds_stereo_params).
 struct StereoParams {
     int pyramid_levels = 0;
     SgmParams sgm;
@@ -67,6 +84,11 @@ struct StereoParams {
     bool filter_spikes = false;
     int speckle_max_region_size = 0;
     bool wide_costs = false;
+    RefineParams refine;
+    DetailParams detail;
+    float occlusion_tolerance = 1.0f;
+    float spike_threshold = 1.0f;
+    float speckle_max_diff = 1.0f;
 };
 
 // depth::RectifiedGeometry (libs/depth/include/einstar/depth/point_image.hpp:12-26).
@@ -160,6 +182,17 @@ private:
         c.filter_spikes = p.filter_spikes;
         c.speckle_max_region_size = p.speckle_max_region_size;
         c.wide_costs = p.wide_costs;
+        c.refine_search_radius = p.refine.search_radius;
+        c.refine_zncc_radius = p.refine.zncc_radius;
+        c.refine_min_zncc = p.refine.min_zncc;
+        c.refine_reject_edge_winners = p.refine.reject_edge_winners;
+        c.detail_radius = p.detail.radius;
+        c.detail_search = p.detail.search;
+        c.detail_step = p.detail.step;
+        c.detail_min_zncc = p.detail.min_zncc;
+        c.occlusion_tolerance = p.occlusion_tolerance;
+        c.spike_threshold = p.spike_threshold;
+        c.speckle_max_diff = p.speckle_max_diff;
         return c;
     }
 

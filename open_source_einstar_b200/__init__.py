@@ -7,8 +7,10 @@ The Python classes mirror the reference's stereo-matcher interface (depth_metal:
 from .stereo import (  # noqa: F401
     INVALID_DISPARITY,
     CudaStereo,
+    DetailParams,
     Errc,
     RectifiedGeometry,
+    RefineParams,
     RemapTable,
     SgmParams,
     StereoError,

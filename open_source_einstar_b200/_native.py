@@ -26,6 +26,10 @@ class StereoParamsC(C.Structure):
         ("pyramid_levels", C.c_int), ("sgm", SgmParamsC), ("subpixel", C.c_int), ("median", C.c_int),
         ("detail_enabled", C.c_int), ("filter_occlusion", C.c_int), ("filter_spikes", C.c_int),
         ("speckle_max_region_size", C.c_int), ("wide_costs", C.c_int),
+        ("refine_search_radius", C.c_int), ("refine_zncc_radius", C.c_int), ("refine_min_zncc", C.c_float),
+        ("refine_reject_edge_winners", C.c_int), ("detail_radius", C.c_int), ("detail_search", C.c_float),
+        ("detail_step", C.c_float), ("detail_min_zncc", C.c_float), ("occlusion_tolerance", C.c_float),
+        ("spike_threshold", C.c_float), ("speckle_max_diff", C.c_float),
     ]
 
 

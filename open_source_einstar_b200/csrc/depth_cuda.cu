@@ -18,6 +18,7 @@
 #include "frame_kernels.cuh"
 #include "fused_kernels.cuh"
 #include "internal.h"
+#include "refine_kernels.cuh"
 
 namespace {
 
@@ -100,6 +101,22 @@ struct ds_handle {
     uint16_t* d_out_u16 = nullptr;
     float* d_out_depth = nullptr;
 
+    // depth::compute_disparity beyond the hot path (pyramid, refinements, filters, speckles): SGM at the
+    // pyramid's coarsest level runs in `sgm`, a hot-path handle of that size; this handle keeps the
+    // rectified pair, the pyramid, the refinement buffers and the outputs.
+    bool refine = false;
+    ds_handle* sgm = nullptr;
+    std::vector<int> lw, lh;                 // level sizes, 0 = the stereo resolution
+    std::vector<uint8_t*> pyr[2];            // levels 1..pyramid_levels (entry 0 unused)
+    float* d_ra = nullptr;                   // disparity ping-pong and confidence, W*H
+    float* d_rb = nullptr;
+    float* d_rconf = nullptr;
+    float* d_rmed = nullptr;                 // median3 of the coarser level
+    uint8_t* d_full[2] = {nullptr, nullptr}; // full-resolution rectified pair (detail refinement)
+    int* d_parent = nullptr;                 // speckle union-find
+    int* d_size = nullptr;
+    int* d_err = nullptr;
+
     ds_geometry geom{};
     float min_depth = 150.0f, max_depth = 700.0f, max_jump = 4.0f;
     bool have_points = false;
@@ -143,6 +160,21 @@ void release(ds_handle* h) {
         f(h->d_costs);
     }
     f(h->d_disp_lr);
+    for (int s = 0; s < 2; ++s) {
+        for (auto* p : h->pyr[s]) f(p);
+        f(h->d_full[s]);
+    }
+    f(h->d_ra);
+    f(h->d_rb);
+    f(h->d_rconf);
+    f(h->d_rmed);
+    f(h->d_parent);
+    f(h->d_size);
+    f(h->d_err);
+    if (h->sgm) {
+        release(h->sgm);
+        delete h->sgm;
+    }
     f(h->d_out_disp);
     f(h->d_out_conf);
     f(h->d_out_u16);
@@ -177,15 +209,29 @@ int validate(const ds_stereo_params& p, int w, int h, std::string& msg) {
         msg = "census window + P2 exceed the 16-bit SGM costs";
         return DS_INVALID_ARGUMENT;
     }
-    if (p.pyramid_levels != 0) {
-        msg = "pyramid + ZNCC refinement is not part of the CUDA hot path (pyramid_levels must be 0)";
-        return DS_UNSUPPORTED;
+    if (p.pyramid_levels < 0 || p.pyramid_levels > 4 || (w >> p.pyramid_levels) < 1 || (h >> p.pyramid_levels) < 1) {
+        msg = "pyramid_levels must be 0..4 with at least one pixel at the coarsest level";
+        return DS_INVALID_ARGUMENT;
     }
-    if (p.detail_enabled || p.filter_occlusion || p.filter_spikes || p.speckle_max_region_size > 0) {
-        msg = "detail refinement, occlusion/spike filters and speckle removal are not part of the CUDA hot path";
-        return DS_UNSUPPORTED;
+    if (p.pyramid_levels > 0 &&
+        (p.refine_zncc_radius < 1 || p.refine_zncc_radius > 15 || p.refine_search_radius < 1 || p.refine_search_radius > 31)) {
+        msg = "refinement: zncc_radius 1..15, search_radius 1..31";
+        return DS_INVALID_ARGUMENT;
+    }
+    if (p.detail_enabled && (p.detail_radius < 1 || p.detail_radius > 32 || !(p.detail_step > 0.0f) || !(p.detail_search >= 0.0f))) {
+        msg = "detail refinement: radius 1..32, step > 0, search >= 0";
+        return DS_INVALID_ARGUMENT;
+    }
+    if (p.speckle_max_region_size < 0 || !(p.speckle_max_diff >= 0.0f)) {
+        msg = "speckle removal: max_region_size and max_diff must be non-negative";
+        return DS_INVALID_ARGUMENT;
     }
     return DS_OK;
+}
+
+// Whether a frame runs depth::compute_disparity's later stages (not only the hot path).
+bool refines(const ds_stereo_params& p) {
+    return p.pyramid_levels > 0 || p.detail_enabled || p.filter_occlusion || p.filter_spikes || p.speckle_max_region_size > 1;
 }
 
 constexpr size_t kMaxSmem = 227 * 1024;
@@ -304,6 +350,7 @@ void free_counted(ds_handle* h, void*& p, size_t bytes) {
 // (Re)allocates the buffers whose size depends on the kernel configuration. The census and the fused
 // slabs carry kGuardRows guard rows above and below (and the census guard columns) for the prefetches.
 void size_config_buffers(ds_handle* h) {
+    if (h->refine) return;  // its SGM buffers belong to h->sgm
     constexpr int g = dsk::kGuardRows;
     h->dp = h->cfg.dp();
     const size_t n = static_cast<size_t>(h->w) * h->h;
@@ -379,48 +426,55 @@ struct StageMarks {
     }
 };
 
-// The whole frame on `st`: [rectify] -> census -> [costs] -> paths -> WTA + L-R -> median + outputs.
-void enqueue_frame(ds_handle* h, const uint8_t* left, const uint8_t* right, bool raw, const ds_outputs& out,
-                   cudaStream_t st) {
-    const uint8_t* img[2] = {left, right};
+StageMarks begin_marks(ds_handle* h, cudaStream_t st) {
     StageMarks marks{h, st};
     if (h->profile) {
         if (h->prof_pending == kProfileRing) throw CudaFailure{cudaErrorNotReady, "profile ring full: call ds_profile_collect"};
         marks.slot = (h->prof_head + h->prof_pending) % kProfileRing;
         ++h->prof_pending;
     }
-    marks.mark(0);
+    return marks;
+}
+
+// Raw pair -> rectified (out_w x out_h) with the handle's tables; `half`: tables at twice the size.
+void enqueue_rectify(ds_handle* h, const uint8_t* const raw[2], uint8_t* const out[2], int out_w, int out_h, int half,
+                     cudaStream_t st) {
+    dsk::RectifyArgs r{};
+    for (int s = 0; s < 2; ++s) {
+        r.raw[s] = raw[s];
+        r.map_x[s] = h->d_map[2 * s];
+        r.map_y[s] = h->d_map[2 * s + 1];
+        r.out[s] = out[s];
+    }
+    r.raw_w = h->raw_w;
+    r.raw_h = h->raw_h;
+    r.map_w = h->map_w;
+    r.out_w = out_w;
+    r.out_h = out_h;
+    r.half = half;
+    dim3 b(32, 8), g((out_w + 32 * dsk::kRectifyPixelsPerThread - 1) / (32 * dsk::kRectifyPixelsPerThread), (out_h + 7) / 8, 2);
+    dsk::k_rectify<<<g, b, 0, st>>>(r);
+    ++g_launches;
+}
+
+// The frame's input pair in h->d_rect: rectified from raw, or copied from the caller's device images.
+void enqueue_inputs(ds_handle* h, const uint8_t* left, const uint8_t* right, bool raw, cudaStream_t st) {
+    const uint8_t* img[2] = {left, right};
     if (raw) {
-        dsk::RectifyArgs r{};
-        for (int s = 0; s < 2; ++s) {
-            r.raw[s] = img[s];
-            r.map_x[s] = h->d_map[2 * s];
-            r.map_y[s] = h->d_map[2 * s + 1];
-            r.out[s] = h->d_rect[s];
-        }
-        r.raw_w = h->raw_w;
-        r.raw_h = h->raw_h;
-        r.map_w = h->map_w;
-        r.out_w = h->w;
-        r.out_h = h->h;
-        r.half = h->map_w == 2 * h->w ? 1 : 0;
-        dim3 b(32, 8), g((h->w + 32 * dsk::kRectifyPixelsPerThread - 1) / (32 * dsk::kRectifyPixelsPerThread), (h->h + 7) / 8, 2);
-        dsk::k_rectify<<<g, b, 0, st>>>(r);
-        ++g_launches;
-        img[0] = h->d_rect[0];
-        img[1] = h->d_rect[1];
+        enqueue_rectify(h, img, h->d_rect, h->w, h->h, h->map_w == 2 * h->w ? 1 : 0, st);
     } else if (left != h->d_rect[0]) {
         // Device inputs of the caller: the path kernel reads the left image as its guide.
         DS_CUDA(cudaMemcpyAsync(h->d_rect[0], left, static_cast<size_t>(h->w) * h->h, cudaMemcpyDeviceToDevice, st));
         DS_CUDA(cudaMemcpyAsync(h->d_rect[1], right, static_cast<size_t>(h->w) * h->h, cudaMemcpyDeviceToDevice, st));
-        img[0] = h->d_rect[0];
-        img[1] = h->d_rect[1];
     }
-    marks.mark(1);
+}
+
+// census -> [costs] -> paths -> WTA + L-R on h->d_rect into h->d_disp_lr; stage marks 2..5.
+void enqueue_sgm(ds_handle* h, StageMarks& marks, cudaStream_t st) {
     {
         dsk::CensusArgs c{};
-        c.img[0] = img[0];
-        c.img[1] = img[1];
+        c.img[0] = h->d_rect[0];
+        c.img[1] = h->d_rect[1];
         c.out[0] = h->d_census[0];
         c.out[1] = h->d_census[1];
         c.w = h->w;
@@ -440,26 +494,148 @@ void enqueue_frame(ds_handle* h, const uint8_t* left, const uint8_t* right, bool
     marks.mark(4);
     launch_wta(h, st);
     marks.mark(5);
-    {
-        dsk::PostArgs q{};
-        q.disp = h->d_disp_lr;
-        q.w = h->w;
-        q.h = h->h;
-        q.median = h->p.median ? 1 : 0;
-        q.min_disp = h->p.sgm.min_disparity;
-        q.out_disp = out.disparity;
-        q.out_conf = out.confidence;
-        q.out_u16 = out.disparity_u16;
-        q.out_depth = h->have_points ? out.depth : nullptr;
-        q.f = h->geom.f;
-        q.baseline = h->geom.baseline;
-        q.cx_offset = h->geom.cx_offset;
-        q.min_depth = h->min_depth;
-        q.max_depth = h->max_depth;
-        dim3 b(32, 8), g((h->w + 31) / 32, (h->h + 7) / 8);
-        dsk::k_post<<<g, b, 0, st>>>(q);
+}
+
+// Median (optional) and the outputs of disparity `disp` (W x H); confidence from `conf` (else 1 where valid).
+void enqueue_post(ds_handle* h, const float* disp, const float* conf, int median, const ds_outputs& out, cudaStream_t st) {
+    dsk::PostArgs q{};
+    q.disp = disp;
+    q.conf_in = conf;
+    q.w = h->w;
+    q.h = h->h;
+    q.median = median;
+    q.min_disp = h->p.sgm.min_disparity;
+    q.out_disp = out.disparity;
+    q.out_conf = out.confidence;
+    q.out_u16 = out.disparity_u16;
+    q.out_depth = h->have_points ? out.depth : nullptr;
+    q.f = h->geom.f;
+    q.baseline = h->geom.baseline;
+    q.cx_offset = h->geom.cx_offset;
+    q.min_depth = h->min_depth;
+    q.max_depth = h->max_depth;
+    dim3 b(32, 8), g((h->w + 31) / 32, (h->h + 7) / 8);
+    dsk::k_post<<<g, b, 0, st>>>(q);
+    ++g_launches;
+}
+
+// depth::compute_disparity (stereo.cpp:501-536): pyramid, SGM at the coarsest level, refine_level up to the
+// stereo resolution, detail refinement (raw frames with tables at twice the size), filters, speckles. Raw
+// frames with tables at twice the size are rectified at full resolution and box-downsampled, as the CPU
+// frontend prepares them (stereo_frontend.cpp:331-335).
+void enqueue_refine(ds_handle* h, const uint8_t* left, const uint8_t* right, bool raw, const ds_outputs& out,
+                    StageMarks& marks, cudaStream_t st) {
+    const auto& p = h->p;
+    const int L = p.pyramid_levels;
+    ds_handle* sg = h->sgm;
+    const int w = h->w, ht = h->h;
+    const size_t n = static_cast<size_t>(w) * ht;
+    const dim3 b2(32, 8);
+    auto grid2 = [](int gw, int gh) { return dim3((gw + 31) / 32, (gh + 7) / 8); };
+    marks.mark(0);
+    const bool full = raw && h->d_full[0] && h->map_w == 2 * w;
+    if (full) {  // the full-resolution pair for the detail refinement, box-downsampled to the stereo resolution
+        const uint8_t* img[2] = {left, right};
+        enqueue_rectify(h, img, h->d_full, 2 * w, 2 * ht, 0, st);
+        for (int s = 0; s < 2; ++s) dsk::k_downsample2<<<grid2(w, ht), b2, 0, st>>>(h->d_full[s], 2 * w, 2 * ht, h->d_rect[s]);
+        g_launches += 2;
+    } else {
+        enqueue_inputs(h, left, right, raw, st);
+    }
+    for (int l = 1; l <= L; ++l)
+        for (int s = 0; s < 2; ++s) {
+            const uint8_t* src = l == 1 ? h->d_rect[s] : h->pyr[s][l - 1];
+            uint8_t* dst = l == L ? sg->d_rect[s] : h->pyr[s][l];
+            dsk::k_downsample2<<<grid2(h->lw[l], h->lh[l]), b2, 0, st>>>(src, h->lw[l - 1], h->lh[l - 1], dst);
+            ++g_launches;
+        }
+    if (L == 0)
+        for (int s = 0; s < 2; ++s) DS_CUDA(cudaMemcpyAsync(sg->d_rect[s], h->d_rect[s], n, cudaMemcpyDeviceToDevice, st));
+    marks.mark(1);
+    enqueue_sgm(sg, marks, st);
+    auto other = [&](const float* c) { return c == h->d_ra ? h->d_rb : h->d_ra; };
+    const float* cur = sg->d_disp_lr;
+    for (int l = L - 1; l >= 0; --l) {
+        dsk::k_median3<<<grid2(h->lw[l + 1], h->lh[l + 1]), b2, 0, st>>>(cur, h->lw[l + 1], h->lh[l + 1], h->d_rmed);
+        dsk::RefineArgs ra{};
+        ra.left = l == 0 ? h->d_rect[0] : h->pyr[0][l];
+        ra.right = l == 0 ? h->d_rect[1] : h->pyr[1][l];
+        ra.coarse = h->d_rmed;
+        ra.w = h->lw[l];
+        ra.h = h->lh[l];
+        ra.cw = h->lw[l + 1];
+        ra.ch = h->lh[l + 1];
+        ra.search_radius = p.refine_search_radius;
+        ra.zncc_radius = p.refine_zncc_radius;
+        ra.min_zncc = p.refine_min_zncc;
+        ra.reject_edge_winners = p.refine_reject_edge_winners ? 1 : 0;
+        ra.subpixel = p.subpixel ? 1 : 0;
+        ra.disp = other(cur);
+        ra.conf = h->d_rconf;
+        dsk::k_refine_level<<<dim3((ra.w + 31) / 32, (ra.h + 3) / 4), dim3(32, 4), 0, st>>>(ra);
+        g_launches += 2;
+        cur = ra.disp;
+    }
+    float* dcur = const_cast<float*>(cur);  // the later stages work in place or ping-pong through d_ra / d_rb
+    if (p.detail_enabled && full) {
+        float* nxt = other(dcur);
+        DS_CUDA(cudaMemcpyAsync(nxt, dcur, n * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        dsk::DetailArgs da{};
+        da.full_left = h->d_full[0];
+        da.full_right = h->d_full[1];
+        da.W = 2 * w;
+        da.H = 2 * ht;
+        da.first = dcur;
+        da.disp = nxt;
+        da.w = w;
+        da.h = ht;
+        da.radius = p.detail_radius;
+        da.K = std::min(16, static_cast<int>(lroundf(p.detail_search / p.detail_step)));
+        da.step = p.detail_step;
+        da.min_zncc = p.detail_min_zncc;
+        da.subpixel = p.subpixel ? 1 : 0;
+        dsk::k_refine_detail<<<dim3((w + 31) / 32, (ht + 3) / 4), dim3(32, 4), 0, st>>>(da);
+        ++g_launches;
+        dcur = nxt;
+    }
+    if (p.filter_occlusion) {
+        dsk::k_filter_occlusion<<<ht, 256, static_cast<size_t>(w) * sizeof(int), st>>>(dcur, w, p.occlusion_tolerance);
         ++g_launches;
     }
+    if (p.filter_spikes) {
+        float* nxt = other(dcur);
+        dsk::k_filter_spikes<<<grid2(w, ht), b2, 0, st>>>(dcur, w, ht, p.spike_threshold, nxt);
+        ++g_launches;
+        dcur = nxt;
+    }
+    if (p.speckle_max_region_size > 1) {
+        const int nn = static_cast<int>(n), bl = (nn + 255) / 256;
+        DS_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(int), st));
+        dsk::k_speckle_init<<<bl, 256, 0, st>>>(dcur, nn, h->d_parent, h->d_size);
+        dsk::k_speckle_union<<<grid2(w, ht), b2, 0, st>>>(dcur, w, ht, p.speckle_max_diff, h->d_parent, h->d_err);
+        dsk::k_speckle_count<<<bl, 256, 0, st>>>(dcur, nn, h->d_parent, h->d_size, h->d_err);
+        dsk::k_speckle_apply<<<bl, 256, 0, st>>>(dcur, nn, h->d_parent, h->d_size, p.speckle_max_region_size, h->d_err);
+        g_launches += 4;
+    }
+    enqueue_post(h, dcur, L > 0 ? h->d_rconf : nullptr, 0, out, st);
+    marks.mark(6);
+    DS_CUDA(cudaGetLastError());
+}
+
+// The whole frame on `st`: [rectify] -> census -> [costs] -> paths -> WTA + L-R -> median + outputs, or
+// depth::compute_disparity's stages when the handle refines.
+void enqueue_frame(ds_handle* h, const uint8_t* left, const uint8_t* right, bool raw, const ds_outputs& out,
+                   cudaStream_t st) {
+    StageMarks marks = begin_marks(h, st);
+    if (h->refine) {
+        enqueue_refine(h, left, right, raw, out, marks, st);
+        return;
+    }
+    marks.mark(0);
+    enqueue_inputs(h, left, right, raw, st);
+    marks.mark(1);
+    enqueue_sgm(h, marks, st);
+    enqueue_post(h, h->d_disp_lr, nullptr, h->p.median ? 1 : 0, out, st);
     marks.mark(6);
     DS_CUDA(cudaGetLastError());
 }
@@ -496,6 +672,11 @@ int run_host(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t 
         if (out->rect_right) DS_CUDA(cudaMemcpyAsync(out->rect_right, h->d_rect[1], n, cudaMemcpyDeviceToHost, h->stream));
     }
     DS_CUDA(cudaStreamSynchronize(h->stream));
+    if (h->refine && h->p.speckle_max_region_size > 1) {
+        int err = 0;
+        DS_CUDA(cudaMemcpy(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) return h->fail(DS_IO, "speckle removal: union-find exceeded its iteration bound");
+    }
     float ms = 0.0f;
     DS_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     h->timings.gpu_ms = ms;
@@ -719,6 +900,36 @@ int create_handle(const ds_stereo_params* params, int width, int height, bool ex
             h->rect_raw[s] = h->alloc<uint8_t>(n + 2 * static_cast<size_t>(dsk::kGuardRows) * width);
             h->d_rect[s] = h->rect_raw[s] + static_cast<size_t>(dsk::kGuardRows) * width;
         }
+        if (refines(*params)) {
+            if (external_volumes) return h->fail(DS_UNSUPPORTED, "the refinement stages run per frame (ds_compute*), "
+                                                                 "not in batches or the request server");
+            h->refine = true;
+            const int L = params->pyramid_levels;
+            h->lw.assign(1, width);
+            h->lh.assign(1, height);
+            for (int l = 1; l <= L; ++l) {
+                h->lw.push_back(h->lw.back() / 2);
+                h->lh.push_back(h->lh.back() / 2);
+            }
+            for (int s = 0; s < 2; ++s) {
+                h->pyr[s].assign(std::max(L, 1), nullptr);
+                for (int l = 1; l < L; ++l) h->pyr[s][l] = h->alloc<uint8_t>(static_cast<size_t>(h->lw[l]) * h->lh[l]);
+            }
+            ds_stereo_params ip = *params;  // the coarsest level: the hot path without the median
+            ip.pyramid_levels = 0;
+            ip.median = 0;
+            ip.detail_enabled = ip.filter_occlusion = ip.filter_spikes = 0;
+            ip.speckle_max_region_size = 0;
+            const int rc = create_handle(&ip, h->lw[L], h->lh[L], false, &h->sgm);
+            if (rc != DS_OK) return h->fail(rc, std::string("SGM level: ") + g_error);
+            h->d_ra = h->alloc<float>(n);
+            h->d_rb = h->alloc<float>(n);
+            h->d_rconf = h->alloc<float>(n);
+            h->d_rmed = h->alloc<float>(n);
+            h->d_parent = h->alloc<int>(n);
+            h->d_size = h->alloc<int>(n);
+            h->d_err = h->alloc<int>(1);
+        }
         size_config_buffers(h);
         h->d_disp_lr = h->alloc<float>(n);
         h->d_out_disp = h->alloc<float>(n);
@@ -742,7 +953,12 @@ int create_handle(const ds_stereo_params* params, int width, int height, bool ex
 namespace ds {
 
 int validate_params(const ds_stereo_params& params, int width, int height, std::string& message) {
-    return validate(params, width, height, message);
+    const int rc = validate(params, width, height, message);
+    if (rc == DS_OK && refines(params)) {
+        message = "the refinement stages run per frame (ds_compute*), not in the request server";
+        return DS_UNSUPPORTED;
+    }
+    return rc;
 }
 
 int create_shared_volume_handle(const ds_stereo_params* params, int width, int height, ds_handle** out) {
@@ -829,6 +1045,17 @@ DS_API void ds_default_params(ds_stereo_params* p) {
     p->sgm.lr_max_diff = 1;
     p->subpixel = 1;
     p->median = 1;
+    p->refine_search_radius = 2;  // depth::RefineParams, DetailParams, FilterParams, SpeckleParams defaults
+    p->refine_zncc_radius = 3;
+    p->refine_min_zncc = 0.5f;
+    p->refine_reject_edge_winners = 1;
+    p->detail_radius = 5;
+    p->detail_search = 1.0f;
+    p->detail_step = 0.5f;
+    p->detail_min_zncc = 0.5f;
+    p->occlusion_tolerance = 1.0f;
+    p->spike_threshold = 1.0f;
+    p->speckle_max_diff = 1.0f;
 }
 
 DS_API const char* ds_last_global_error(void) { return g_error.c_str(); }
@@ -878,6 +1105,8 @@ DS_API int ds_set_rectification(ds_handle* h, const float* lx, const float* ly, 
         const float* src[4] = {lx, ly, rx, ry};
         for (int i = 0; i < 4; ++i) DS_CUDA(cudaMemcpyAsync(h->d_map[i], src[i], n * 4, cudaMemcpyHostToDevice, h->stream));
         DS_CUDA(cudaStreamSynchronize(h->stream));
+        if (h->refine && twice && !h->d_full[0])  // full-resolution rectified pair (downsampled; detail refinement)
+            for (auto*& q : h->d_full) q = h->alloc<uint8_t>(static_cast<size_t>(map_w) * map_h);
         h->map_w = map_w;
         h->map_h = map_h;
         h->raw_w = raw_w;
@@ -944,6 +1173,7 @@ DS_API const char* ds_last_error(const ds_handle* h) { return h ? h->err.c_str()
 
 DS_API int ds_debug_read(ds_handle* h, uint64_t* census_left, uint64_t* census_right, uint16_t* path_sums) {
     if (!h) return DS_INVALID_ARGUMENT;
+    if (h->refine) return h->fail(DS_UNSUPPORTED, "intermediate reads cover the hot path only");
     return guarded(h, [&]() -> int {
         const size_t n = static_cast<size_t>(h->w) * h->h;
         DS_CUDA(cudaStreamSynchronize(h->stream));
@@ -1013,7 +1243,7 @@ DS_API int ds_debug_read(ds_handle* h, uint64_t* census_left, uint64_t* census_r
     });
 }
 
-DS_API size_t ds_device_bytes(const ds_handle* h) { return h ? h->bytes : 0; }
+DS_API size_t ds_device_bytes(const ds_handle* h) { return h ? h->bytes + (h->sgm ? h->sgm->bytes : 0) : 0; }
 
 DS_API int ds_profile_enable(ds_handle* h, int on) {
     if (!h) return DS_INVALID_ARGUMENT;
@@ -1055,6 +1285,11 @@ DS_API uint64_t ds_kernel_launches(void) { return g_launches.load(); }
 DS_API int ds_set_kernel_config(ds_handle* h, const ds_kernel_config* c) {
     if (!h) return DS_INVALID_ARGUMENT;
     if (!c) return h->fail(DS_INVALID_ARGUMENT, "null kernel config");
+    if (h->refine) {  // the SGM level's kernels
+        const int rc = ds_set_kernel_config(h->sgm, c);
+        if (rc != DS_OK) h->err = h->sgm->err;
+        return rc;
+    }
     if (!ds::cfg_supported(c->regs_per_lane, c->lanes_per_line))
         return h->fail(DS_INVALID_ARGUMENT,
                        "unsupported kernel configuration (lanes per line 8: R 4,6,8; 16: R 1-4; 32: R 1,2,3,4,6,8)");
@@ -1090,6 +1325,7 @@ DS_API int ds_set_kernel_config(ds_handle* h, const ds_kernel_config* c) {
 
 DS_API int ds_get_kernel_config(const ds_handle* h, ds_kernel_config* c) {
     if (!h || !c) return DS_INVALID_ARGUMENT;
+    if (h->refine) return ds_get_kernel_config(h->sgm, c);  // the SGM level's kernels
     c->regs_per_lane = h->cfg.R;
     c->lanes_per_line = h->cfg.seg;
     c->materialize_costs = h->cfg.materialize ? 1 : 0;

@@ -149,6 +149,7 @@ __global__ void k_census(CensusArgs a) {
 
 struct PostArgs {
     const float* disp;
+    const float* conf_in;  // confidence of valid pixels (refinement: the ZNCC score); null: 1
     int w, h, median, min_disp;
     float* out_disp;
     float* out_conf;
@@ -184,7 +185,7 @@ __device__ __forceinline__ void post_body(const PostArgs& a, int bx, int by) {
     }
     const bool ok = valid_disparity(d);
     if (a.out_disp) a.out_disp[i] = d;
-    if (a.out_conf) a.out_conf[i] = ok ? 1.0f : 0.0f;
+    if (a.out_conf) a.out_conf[i] = ok ? (a.conf_in ? a.conf_in[i] : 1.0f) : 0.0f;
     if (a.out_u16) {
         uint16_t u = 0xFFFFu;
         if (ok) {

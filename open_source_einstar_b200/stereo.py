@@ -62,9 +62,28 @@ class SgmParams:
 
 
 @dataclass
+class RefineParams:
+    """depth::RefineParams (libs/depth/include/einstar/depth/stereo.hpp:41-47)."""
+    search_radius: int = 2
+    zncc_radius: int = 3
+    min_zncc: float = 0.5
+    reject_edge_winners: bool = True
+
+
+@dataclass
+class DetailParams:
+    """depth::DetailParams (stereo.hpp:53-61) without `enabled` (StereoParams.detail_enabled)."""
+    radius: int = 5
+    search: float = 1.0
+    step: float = 0.5
+    min_zncc: float = 0.5
+
+
+@dataclass
 class StereoParams:
-    """depth::StereoParams reduced to the hot path (pyramid 0, subpixel, median). The later stages keep
-    their switches; asking for them raises StereoError(unsupported), as the C ABI returns."""
+    """depth::StereoParams. The defaults are the hot path (pyramid 0, later stages off, subpixel, median).
+    pyramid_levels > 0, detail_enabled, the filters or speckle_max_region_size > 1 select the full
+    depth::compute_disparity (ZNCC refinement, detail, filters, speckles) instead; see ds_stereo_params."""
     pyramid_levels: int = 0
     sgm: SgmParams = field(default_factory=SgmParams)
     subpixel: bool = True
@@ -74,6 +93,16 @@ class StereoParams:
     filter_spikes: bool = False
     speckle_max_region_size: int = 0
     wide_costs: bool = False
+    refine: RefineParams = field(default_factory=RefineParams)
+    detail: DetailParams = field(default_factory=DetailParams)
+    occlusion_tolerance: float = 1.0
+    spike_threshold: float = 1.0
+    speckle_max_diff: float = 1.0
+
+    @property
+    def refines(self) -> bool:
+        return bool(self.pyramid_levels > 0 or self.detail_enabled or self.filter_occlusion or self.filter_spikes
+                    or self.speckle_max_region_size > 1)
 
     def c(self) -> N.StereoParamsC:
         s = self.sgm
@@ -84,7 +113,10 @@ class StereoParams:
                          float(s.uniqueness), s.lr_max_diff),
             int(bool(self.subpixel)), int(bool(self.median)), int(bool(self.detail_enabled)),
             int(bool(self.filter_occlusion)), int(bool(self.filter_spikes)), int(self.speckle_max_region_size),
-            int(bool(self.wide_costs)))
+            int(bool(self.wide_costs)), int(self.refine.search_radius), int(self.refine.zncc_radius),
+            float(self.refine.min_zncc), int(bool(self.refine.reject_edge_winners)), int(self.detail.radius),
+            float(self.detail.search), float(self.detail.step), float(self.detail.min_zncc),
+            float(self.occlusion_tolerance), float(self.spike_threshold), float(self.speckle_max_diff))
 
 
 @dataclass
@@ -180,7 +212,8 @@ class CudaStereo:
         s = cls(h.value, params, int(width), int(height))
         if tuned:
             from .autotune import apply, tuned_config
-            cfg = tuned_config(width, height, params)
+            lv = params.pyramid_levels if params.refines else 0  # SGM runs at the pyramid's coarsest level
+            cfg = tuned_config(int(width) >> lv, int(height) >> lv, params)
             if cfg:
                 apply(s, cfg)
         return s

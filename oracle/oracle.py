@@ -196,8 +196,34 @@ class Port:
         return _pipeline(self, left, right, p, subpixel, median, geometry, min_depth, max_depth, maps)
 
 
+class _RefStereo(C.Structure):
+    """ref_stereo_params of oracle/ref_shim.cpp (depth::StereoParams, stereo.hpp:41-88)."""
+    _fields_ = [("pyramid_levels", C.c_int), ("sgm", _Sgm), ("refine_search_radius", C.c_int),
+                ("refine_zncc_radius", C.c_int), ("refine_min_zncc", C.c_float), ("refine_reject_edge_winners", C.c_int),
+                ("detail_enabled", C.c_int), ("detail_radius", C.c_int), ("detail_search", C.c_float),
+                ("detail_step", C.c_float), ("detail_min_zncc", C.c_float), ("filter_occlusion", C.c_int),
+                ("filter_occlusion_tolerance", C.c_float), ("filter_spikes", C.c_int), ("filter_spike_threshold", C.c_float),
+                ("speckle_max_region_size", C.c_int), ("speckle_max_diff", C.c_float), ("subpixel", C.c_int)]
+
+
+def ref_stereo_params(sp) -> _RefStereo:
+    """From the package's StereoParams (field names of depth::StereoParams)."""
+    g = sp.sgm
+    sgm = OracleSgm(min_disparity=g.min_disparity, num_disparities=g.num_disparities, census_radius_x=g.census_radius_x,
+                    census_radius_y=g.census_radius_y, p1=g.p1, p2=g.p2, adaptive_p2=g.adaptive_p2,
+                    eight_paths=g.eight_paths, slant_steps=g.slant_steps, uniqueness=g.uniqueness,
+                    lr_max_diff=g.lr_max_diff).c()
+    return _RefStereo(int(sp.pyramid_levels), sgm, int(sp.refine.search_radius), int(sp.refine.zncc_radius),
+                      float(sp.refine.min_zncc), int(bool(sp.refine.reject_edge_winners)), int(bool(sp.detail_enabled)),
+                      int(sp.detail.radius), float(sp.detail.search), float(sp.detail.step), float(sp.detail.min_zncc),
+                      int(bool(sp.filter_occlusion)), float(sp.occlusion_tolerance), int(bool(sp.filter_spikes)),
+                      float(sp.spike_threshold), int(sp.speckle_max_region_size), float(sp.speckle_max_diff),
+                      int(bool(sp.subpixel)))
+
+
 class Ref(Port):
-    """The reference's own stereo.cpp (oracle/_ref) for census / sgm_disparity / median3."""
+    """The reference's own stereo.cpp (oracle/_ref): census, sgm_disparity, median3, downsample2, the refinement
+    stages and compute_disparity."""
 
     def __init__(self, path: str = REF_SO, port_path: str = PORT_SO):
         super().__init__(port_path)
@@ -210,6 +236,13 @@ class Ref(Port):
         R.ref_sgm_disparity.argtypes = [vp, vp, i, i, C.POINTER(_Sgm), i, vp]
         R.ref_median3.argtypes = [vp, i, i, vp]
         R.ref_threads.restype = i
+        P = C.POINTER(_RefStereo)
+        R.ref_downsample2.argtypes = [vp, i, i, vp]
+        R.ref_refine_level.argtypes = [vp, vp, i, i, vp, i, i, P, vp, vp]
+        R.ref_refine_detail.argtypes = [vp, vp, i, i, vp, i, i, P]
+        R.ref_filter_disparity.argtypes = [vp, i, i, P]
+        R.ref_remove_speckles.argtypes = [vp, i, i, P]
+        R.ref_compute_disparity.argtypes = [vp, vp, i, i, vp, vp, P, vp, vp]
 
     @staticmethod
     def available() -> bool:
@@ -238,6 +271,37 @@ class Ref(Port):
         out = np.empty_like(d)
         self.ref.ref_median3(_p(d), w, h, _p(out))
         return out
+
+    def downsample2(self, img) -> np.ndarray:
+        img = _u8(img)
+        h, w = img.shape
+        out = np.empty((h // 2, w // 2), np.uint8)
+        self.ref.ref_downsample2(_p(img), w, h, _p(out))
+        return out
+
+    def filter_disparity(self, disp, sp) -> np.ndarray:
+        d = np.array(disp, np.float32, order="C")
+        h, w = d.shape
+        self.ref.ref_filter_disparity(_p(d), w, h, C.byref(ref_stereo_params(sp)))
+        return d
+
+    def remove_speckles(self, disp, sp) -> np.ndarray:
+        d = np.array(disp, np.float32, order="C")
+        h, w = d.shape
+        self.ref.ref_remove_speckles(_p(d), w, h, C.byref(ref_stereo_params(sp)))
+        return d
+
+    def compute_disparity(self, left, right, sp, full_left=None, full_right=None):
+        """depth::compute_disparity (stereo.cpp:501-536): (disparity, confidence)."""
+        left, right = _u8(left), _u8(right)
+        h, w = left.shape
+        fl = None if full_left is None else _u8(full_left)
+        fr = None if full_right is None else _u8(full_right)
+        disp = np.empty((h, w), np.float32)
+        conf = np.empty((h, w), np.float32)
+        self.ref.ref_compute_disparity(_p(left), _p(right), w, h, None if fl is None else _p(fl),
+                                       None if fr is None else _p(fr), C.byref(ref_stereo_params(sp)), _p(disp), _p(conf))
+        return disp, conf
 
 
 def _pipeline(o, left, right, p, subpixel, median, geometry, min_depth, max_depth, maps):

@@ -61,10 +61,24 @@ int main(int argc, char** argv) {
     depth_cuda::StereoParams big = p;
     big.sgm.num_disparities = 600;
     if (auto c = depth_cuda::CudaStereo::create(big, w, h); c || c.error().code != depth_cuda::Errc::invalid_argument) bad = 1;
-    // a stage off the hot path: unsupported
+    // depth::compute_disparity's refinement: one pyramid level runs; five are out of range
     depth_cuda::StereoParams pyr = p;
     pyr.pyramid_levels = 1;
-    if (auto c = depth_cuda::CudaStereo::create(pyr, w, h); c || c.error().code != depth_cuda::Errc::unsupported) bad = 1;
+    pyr.sgm.min_disparity = p.sgm.min_disparity / 2 - 2;
+    pyr.sgm.num_disparities = p.sgm.num_disparities / 2 + 4;
+    pyr.filter_spikes = true;
+    pyr.speckle_max_region_size = 20;
+    if (auto c = depth_cuda::CudaStereo::create(pyr, w, h); !c) {
+        bad = 1;
+    } else if (auto res = (*c)->compute(l, r); !res) {
+        bad = 1;
+    } else {
+        std::size_t valid = 0;
+        for (std::size_t i = 0; i < n; ++i) valid += res->disparity[i] > -1.0e8f && res->confidence[i] > 0.0f;
+        if (valid == 0) bad = 1;
+    }
+    pyr.pyramid_levels = 5;
+    if (auto c = depth_cuda::CudaStereo::create(pyr, w, h); c || c.error().code != depth_cuda::Errc::invalid_argument) bad = 1;
     // compute_raw before set_rectification: invalid_argument (metal_stereo.cpp:343)
     if (auto res = (*s)->compute_raw(l, r); res || res.error().code != depth_cuda::Errc::invalid_argument) bad = 1;
     std::printf(bad ? "FAIL\n" : "OK\n");

@@ -75,13 +75,22 @@ def test_create_rejects_like_metal(lib, change, code, msg):
     assert int(e.value.code) == code and msg in e.value.message
 
 
-@pytest.mark.parametrize("change", [dict(pyramid_levels=2), dict(detail_enabled=True), dict(filter_occlusion=True),
-                                    dict(filter_spikes=True), dict(speckle_max_region_size=200)])
-def test_stages_off_the_hot_path_are_unsupported(lib, change):
-    from open_source_einstar_b200 import CudaStereo, Errc, StereoError, StereoParams
+@pytest.mark.parametrize("change", [dict(pyramid_levels=5), dict(pyramid_levels=-1),
+                                    dict(pyramid_levels=1, refine=dict(zncc_radius=0)),
+                                    dict(pyramid_levels=1, refine=dict(search_radius=40)),
+                                    dict(detail_enabled=True, detail=dict(step=0.0)),
+                                    dict(speckle_max_region_size=-3)])
+def test_refinement_parameters_are_validated(lib, change):
+    """The stages of depth::compute_disparity beyond the hot path are checked before any device call."""
+    from open_source_einstar_b200 import CudaStereo, DetailParams, Errc, RefineParams, StereoError, StereoParams
+    kw = dict(change)
+    if "refine" in kw:
+        kw["refine"] = RefineParams(**kw["refine"])
+    if "detail" in kw:
+        kw["detail"] = DetailParams(**kw["detail"])
     with pytest.raises(StereoError) as e:
-        CudaStereo.create(StereoParams(**change), 64, 48)
-    assert e.value.code == Errc.unsupported
+        CudaStereo.create(StereoParams(**kw), 64, 48)
+    assert e.value.code == Errc.invalid_argument
 
 
 def test_bad_sizes(lib):
