@@ -455,6 +455,129 @@ def run_offline(args, world, rank, local):
     return 0
 
 
+def frontend_params(f, baseline):
+    """The scanner frontend's depth::StereoParams (stereo_frontend.cpp:21-34): stereo on the half-resolution
+    rectified pair, SGM a level below over the quarter-resolution disparities of 150-700 mm (+/- 2 px
+    guard), the reference's refinement, detail, filter and speckle defaults."""
+    import math
+    from open_source_einstar_b200 import SgmParams, StereoParams
+    fq = f / 4.0
+    d_max, d_min = fq * baseline / 150.0, fq * baseline / 700.0
+    sgm = SgmParams(min_disparity=int(math.floor(d_min)) - 2, num_disparities=int(math.ceil(d_max - d_min)) + 4)
+    return StereoParams(pyramid_levels=1, sgm=sgm, median=False, detail_enabled=True, filter_occlusion=True,
+                        filter_spikes=True, speckle_max_region_size=200)
+
+
+def reference_frontend_frame(ref, pair, sp):
+    """The CPU frontend's depth step on one raw pair (stereo_frontend.cpp:331-335): remap both images at
+    full resolution, box-downsample, depth::compute_disparity with the full-resolution pair (oracle/_ref)."""
+    (lx, ly), (rx, ry) = pair.maps
+    t0 = time.perf_counter()
+    fl, fr = ref.remap(pair.left, lx, ly), ref.remap(pair.right, rx, ry)
+    d, c = ref.compute_disparity(ref.downsample2(fl), ref.downsample2(fr), sp, fl, fr)
+    return time.perf_counter() - t0, d, c
+
+
+def run_frontend(args, world, rank, local):
+    """The scanner frontend's whole depth step (depth::compute_disparity as stereo_frontend.cpp configures
+    it) on raw 1280x1024 pairs: full-resolution GPU remap, box downsample to 640x512, SGM at 320x256,
+    slanted ZNCC refinement to 640x512, detail refinement on the 1280x1024 pair, occlusion and spike
+    filters, speckle removal. One step = --frames frames; metric frames/s."""
+    import torch
+    from open_source_einstar_b200 import CudaStereo, RemapTable
+    from open_source_einstar_b200.stereo import STAGE_NAMES, kernel_launches
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    B = args.frames
+    pairs = make_frames(B, 100 * rank, dev)
+    (lx, ly), (rx, ry) = pairs[0].maps
+    sp = frontend_params(pairs[0].f, pairs[0].baseline)
+    w, h = W // 2, H // 2
+    s = CudaStereo.create(sp, w, h)
+    s.set_rectification(RemapTable(lx, ly), RemapTable(rx, ry), W, H)
+    raw = [(torch.from_numpy(p.left).to(dev), torch.from_numpy(p.right).to(dev)) for p in pairs]
+    outs = [{"disparity": torch.empty((h, w), dtype=torch.float32, device=dev),
+             "confidence": torch.empty((h, w), dtype=torch.float32, device=dev)} for _ in range(B)]
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+
+    def step():
+        for (l, r), o in zip(raw, outs):
+            s.compute_device(l, r, o, stream=stream, raw=True)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    # the device results equal the host API's (which the parity tests hold to the reference)
+    r0 = s.compute_raw(pairs[0].left, pairs[0].right)
+    if not np.array_equal(r0.disparity.view(np.uint32), outs[0]["disparity"].cpu().numpy().view(np.uint32)):
+        raise SystemExit("device-resident and host frames differ")
+    clk = ClockSampler(local).__enter__()
+    s.profile(True)
+    s.profile_collect()
+    l0 = kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    launches = kernel_launches() - l0
+    ms = e0.elapsed_time(e1)
+    stages = s.profile_collect(max_frames=B * args.steps + 8)
+    s.profile(False)
+    n_frames = B * args.steps
+    # end to end through the host API: raw pair in from host memory, disparity + confidence back
+    host = [(np.ascontiguousarray(p.left), np.ascontiguousarray(p.right)) for p in pairs]
+    res = [s.compute_raw(*host[0])]
+    t0 = time.perf_counter()
+    for i in range(n_frames):
+        res[0] = s.compute_raw(*host[i % B])
+    e2e_s = time.perf_counter() - t0
+    clk.__exit__(None, None, None)
+    s.close()
+    frame_tot = stages.sum(axis=1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle.oracle import Ref
+        ref = Ref()
+        cpu_pairs = make_frames(2, 0, dev)
+        reference_frontend_frame(ref, cpu_pairs[0], sp)
+        times = []
+        t_start = time.perf_counter()
+        while len(times) < 8 and time.perf_counter() - t_start < 20.0:
+            times.append(reference_frontend_frame(ref, cpu_pairs[len(times) % 2], sp)[0])
+        med = statistics.median(times)
+        cpu = {"value": 1e3 / (med * 1e3), "unit": "frames/s", "cores": ref.threads(), "kind": "reference",
+               "ms_per_frame": med * 1e3,
+               "sample": f"{len(times)} raw 1280x1024 frames: restated calib::remap x2, the reference's downsample2 and "
+                         "compute_disparity (oracle/_ref: libs/depth/src/stereo.cpp) over "
+                         f"{ref.threads()} threads"}
+    if rank == 0:
+        line = {"metric": "frontend depth frames/s (depth::compute_disparity as the scanner frontend runs it), raw 1280x1024",
+                "workload": "frontend", "value": n_frames / (ms * 1e-3), "unit": "frames/s", "higher_is_better": True,
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "ms_per_frame": ms / n_frames, "dtype": "u8/f32/f64", "data": "synthetic", "vs_baseline": None,
+                "scaling": "weak",
+                "frame_ms": {"p50": float(np.percentile(frame_tot, 50)), "p99": float(np.percentile(frame_tot, 99))},
+                "stage_ms": {"rectify_downsample": float(stages[:, 0].mean()),
+                             "sgm_320x256": float(stages[:, 1:5].sum(axis=1).mean()),
+                             "refine_detail_filters_speckles": float(stages[:, 5].mean())},
+                "config": {"workload": "raw 1280x1024 u8 pairs (config-2 scenes): GPU remap at 1280x1024, 2x2 box to 640x512, "
+                                       f"SGM 4 paths at 320x256 D={sp.sgm.num_disparities}, ZNCC refinement (7x7 slanted, "
+                                       "+/-2 px in 0.5 px) to 640x512, detail refinement (10x10 at 1280x1024), occlusion + "
+                                       "spike filters, speckles < 200 px removed",
+                           "frames_per_step": B, "parallelism": f"replicas x{world}"},
+                "e2e": {"value": n_frames / e2e_s, "unit": "frames/s", "h2d_bytes_per_step": B * 2 * W * H,
+                        "d2h_bytes_per_step": B * w * h * 8,
+                        "api": "CudaStereo.compute_raw (ds_compute_raw): host raw pair in, host disparity + confidence out, "
+                               "wall clock"},
+                "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -465,7 +588,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--reference-budget", type=float, default=150.0, help="seconds of timed reference work at most")
     ap.add_argument("--kernel-config", default="", help="R,SEG,MATERIALIZE override (default: the library's choice)")
-    ap.add_argument("--workload", default="frames", choices=["frames", "serving", "batch64", "offline"],
+    ap.add_argument("--workload", default="frames", choices=["frames", "serving", "batch64", "offline", "frontend"],
                     help="frames: the 1280x1024 D=128 throughput line (default); serving: the request-server latency run")
     ap.add_argument("--duration", type=float, default=20.0, help="serving: seconds of arrivals per rate")
     ap.add_argument("--rates", type=float, nargs="+", default=[120.0, 240.0, 480.0], help="serving: arrival rates (Hz)")
@@ -482,6 +605,8 @@ def main():
         return run_batch64(args, world, rank, local)
     if args.workload == "offline":
         return run_offline(args, world, rank, local)
+    if args.workload == "frontend":
+        return run_frontend(args, world, rank, local)
 
     import torch
     from open_source_einstar_b200 import (CudaStereo, PairDesc, RectifiedGeometry, RemapTable, SgmParams, StereoBatch,

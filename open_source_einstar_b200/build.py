@@ -15,8 +15,10 @@ CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIB_DIR, "libdepth_cuda.so")
 
+# -fmad=false: every float operation of this library is meant to round separately, as the reference's x86-64
+# build evaluates it; no plain multiply and add may be contracted into a fused multiply-add.
 NVCC_FLAGS = [
-    "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
+    "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-fmad=false",
     "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared", "-cudart", "static",
 ]
 

@@ -54,16 +54,18 @@ static __global__ void k_median3(const float* __restrict__ in, int w, int h, flo
     out[i] = d;
 }
 
+// The window sums of a ZNCC score. The reference accumulates all five in double, sample by sample. Sums over
+// the left window (sa, saa) are sums of integers below 2^53, exact in any order, so they are summed once per
+// pixel in integers; the three sums that involve the bilinear right samples (sb, sbb, sab) keep the
+// reference's order and rounding.
 struct ZnccSums {
-    double sa = 0, sb = 0, saa = 0, sbb = 0, sab = 0;
+    double sb = 0, sbb = 0, sab = 0;
     __device__ __forceinline__ void add(double ia, double ib) {
-        sa = __dadd_rn(sa, ia);
         sb = __dadd_rn(sb, ib);
-        saa = __dadd_rn(saa, __dmul_rn(ia, ia));
         sbb = __dadd_rn(sbb, __dmul_rn(ib, ib));
         sab = __dadd_rn(sab, __dmul_rn(ia, ib));
     }
-    __device__ __forceinline__ float score(double n) const {
+    __device__ __forceinline__ float score(double sa, double saa, double n) const {
         const double va = __dsub_rn(saa, __ddiv_rn(__dmul_rn(sa, sa), n));
         const double vb = __dsub_rn(sbb, __ddiv_rn(__dmul_rn(sb, sb), n));
         if (va < 1e-6 || vb < 1e-6) return -1.0f;
@@ -71,34 +73,150 @@ struct ZnccSums {
     }
 };
 
-// One bilinear sample of the right row at xb: rb[x0] (1 - f) + rb[x0 + 1] f in float, as a double; false
-// when x0 or x0 + 1 leave the row.
+// Sum and sum of squares of an n x m byte window (rows `stride` apart), as exact doubles.
+__device__ __forceinline__ void window_moments(const uint8_t* a, size_t stride, int n, int m, double& sa, double& saa) {
+    int s1 = 0, s2 = 0;
+    for (int j = 0; j < m; ++j) {
+        const uint8_t* row = a + static_cast<size_t>(j) * stride;
+        for (int i = 0; i < n; ++i) {
+            const int v = row[i];
+            s1 += v;
+            s2 += v * v;
+        }
+    }
+    sa = static_cast<double>(s1);
+    saa = static_cast<double>(s2);
+}
+
+// Integer-to-float conversions and floor() run on the SM's conversion unit, a quarter of the FMA rate, and
+// would bound the ZNCC loops (several per sample). The samples below convert on the FMA and ALU pipes
+// instead, with the same values:
+// - a byte v as a float: the float with bits 0x4B000000 | v is 2^23 + v, exactly; subtract 2^23;
+// - a byte as a double: likewise with 2^52;
+// - floor(xb) for |xb| < 2^22: xb + 1.5 * 2^23 lies in [2^23, 2^24), where the float spacing is 1, so the
+//   sum is xb rounded to an integer (then one less where that rounded up), and its low mantissa bits
+//   hold that integer. A larger |xb| puts the sample outside any image row (at most 16384 wide), which
+//   the reference also rejects.
+__device__ __forceinline__ float byte_to_float(uint32_t v) { return __fsub_rn(__uint_as_float(0x4B000000u | v), 8388608.0f); }
+__device__ __forceinline__ double byte_to_double(uint32_t v) {
+    return __dsub_rn(__hiloint2double(0x43300000, static_cast<int>(v)), 4503599627370496.0);
+}
+
+// One bilinear sample of the right row at xb, float(rb[x0] (1 - f) + rb[x0 + 1] f) with x0 = floor(xb) and
+// f = xb - x0, as a double; false when x0 or x0 + 1 leave the row (stereo.cpp:110-114).
 __device__ __forceinline__ bool sample_row(const uint8_t* rb, int bw, float xb, double& ib) {
-    const int x0 = static_cast<int>(floorf(xb));
+    if (!(fabsf(xb) < 4194304.0f)) return false;
+    const float t = __fadd_rn(xb, 12582912.0f);
+    float fl = __fsub_rn(t, 12582912.0f);
+    int x0 = __float_as_int(t) - 0x4B400000;
+    if (fl > xb) {
+        fl = __fsub_rn(fl, 1.0f);
+        --x0;
+    }
     if (x0 < 0 || x0 + 1 >= bw) return false;
-    const float f = __fsub_rn(xb, static_cast<float>(x0));
-    ib = static_cast<double>(__fadd_rn(__fmul_rn(static_cast<float>(rb[x0]), __fsub_rn(1.0f, f)),
-                                       __fmul_rn(static_cast<float>(rb[x0 + 1]), f)));
+    const float f = __fsub_rn(xb, fl);
+    ib = static_cast<double>(__fadd_rn(__fmul_rn(byte_to_float(rb[x0]), __fsub_rn(1.0f, f)),
+                                       __fmul_rn(byte_to_float(rb[x0 + 1]), f)));
     return true;
 }
 
-// zncc_slanted (stereo.cpp:102-126).
-__device__ float zncc_slanted(const uint8_t* a, const uint8_t* b, int w, int x, int y, float d, float gx, float gy, int r) {
+// zncc_slanted (stereo.cpp:102-126). Loop counters are carried as floats too (small integers, exact).
+__device__ float zncc_slanted(const uint8_t* a, const uint8_t* b, int w, int x, int y, float d, float gx, float gy, int r,
+                              double sa, double saa) {
     ZnccSums s;
     const int n = (2 * r + 1) * (2 * r + 1);
-    for (int v = -r; v <= r; ++v) {
-        const uint8_t* ra = a + static_cast<size_t>(y + v) * w;
+    const float fr = static_cast<float>(r), fx = static_cast<float>(x);
+    float fv = -fr;
+    for (int v = -r; v <= r; ++v, fv = __fadd_rn(fv, 1.0f)) {
+        const uint8_t* ra = a + static_cast<size_t>(y + v) * w + x;
         const uint8_t* rb = b + static_cast<size_t>(y + v) * w;
-        for (int u = -r; u <= r; ++u) {
-            const float shift = __fadd_rn(__fadd_rn(d, __fmul_rn(gx, static_cast<float>(u))), __fmul_rn(gy, static_cast<float>(v)));
-            const float xb = __fsub_rn(static_cast<float>(x + u), shift);
+        const float gyv = __fmul_rn(gy, fv);
+        float fu = -fr;
+        for (int u = -r; u <= r; ++u, fu = __fadd_rn(fu, 1.0f)) {
+            const float shift = __fadd_rn(__fadd_rn(d, __fmul_rn(gx, fu)), gyv);
+            const float xb = __fsub_rn(__fadd_rn(fx, fu), shift);
             double ib;
             if (!sample_row(rb, w, xb, ib)) return kZnccNoWindow;
-            s.add(static_cast<double>(ra[x + u]), ib);
+            s.add(byte_to_double(ra[u]), ib);
         }
     }
-    return s.score(static_cast<double>(n));
+    return s.score(sa, saa, static_cast<double>(n));
 }
+
+// ---- two candidates at once on the f32x2 pipe --------------------------------------------------------------
+// Blackwell executes a pair of float adds as one instruction (__fadd2_rn), each component rounded as the
+// scalar add. The ZNCC loops below evaluate two candidate disparities per sample that way and share the left
+// sample and its conversion. Products stay scalar (__fmul_rn): a pair multiply followed by a pair add was
+// measured to come out fused (one rounding, the last bit off the reference's) in some kernels despite
+// explicit rounding, while scalar products into pair adds matched the scalar path on every sample tried.
+// The pair loops take no range checks: callers use them only where a bound on the whole window
+// (window_inside) puts every sample inside the right row. floor() is one round-down add: xb + 1.5 * 2^23
+// rounded down is floor(xb) + 1.5 * 2^23 for |xb| < 2^22.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 add2_rn(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 add2_rm(float2 a, float2 b) { return __fadd2_rd(a, b); }
+__device__ __forceinline__ float2 mul2_scalar(float2 a, float2 b) { return f2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)); }
+
+__device__ __forceinline__ float2 bilinear_pair(const uint8_t* rb, float2 xb) {
+    const float2 t = add2_rm(xb, f2(12582912.0f, 12582912.0f));
+    const float2 fl = add2_rn(t, f2(-12582912.0f, -12582912.0f));
+    const float2 f = add2_rn(xb, neg2(fl));
+    const int xa = __float_as_int(t.x) - 0x4B400000, xc = __float_as_int(t.y) - 0x4B400000;
+    const float2 b0 = add2_rn(f2(__uint_as_float(0x4B000000u | rb[xa]), __uint_as_float(0x4B000000u | rb[xc])),
+                                 f2(-8388608.0f, -8388608.0f));
+    const float2 b1 = add2_rn(f2(__uint_as_float(0x4B000000u | rb[xa + 1]), __uint_as_float(0x4B000000u | rb[xc + 1])),
+                                 f2(-8388608.0f, -8388608.0f));
+    return add2_rn(mul2_scalar(b0, add2_rn(f2(1.0f, 1.0f), neg2(f))), mul2_scalar(b1, f));
+}
+
+// zncc_slanted for the disparities d.x and d.y.
+__device__ float2 zncc_slanted_pair(const uint8_t* a, const uint8_t* b, int w, int x, int y, float2 d, float gx, float gy, int r,
+                                    double sa, double saa) {
+    ZnccSums s0, s1;
+    const float fr = static_cast<float>(r), fx = static_cast<float>(x);
+    float fv = -fr;
+    for (int v = -r; v <= r; ++v, fv = __fadd_rn(fv, 1.0f)) {
+        const uint8_t* ra = a + static_cast<size_t>(y + v) * w + x;
+        const uint8_t* rb = b + static_cast<size_t>(y + v) * w;
+        const float gyv = __fmul_rn(gy, fv);
+        float fu = -fr;
+        for (int u = -r; u <= r; ++u, fu = __fadd_rn(fu, 1.0f)) {
+            const float gxu = __fmul_rn(gx, fu), xu = __fadd_rn(fx, fu);
+            const float2 shift = add2_rn(add2_rn(d, f2(gxu, gxu)), f2(gyv, gyv));
+            const float2 ib = bilinear_pair(rb, add2_rn(f2(xu, xu), neg2(shift)));
+            const double ia = byte_to_double(ra[u]);
+            s0.add(ia, static_cast<double>(ib.x));
+            s1.add(ia, static_cast<double>(ib.y));
+        }
+    }
+    const double n = static_cast<double>((2 * r + 1) * (2 * r + 1));
+    return f2(s0.score(sa, saa, n), s1.score(sa, saa, n));
+}
+
+// True when every sample x0 = floor(xb) of a window has 0 <= x0 and x0 + 1 < width, for xb between lo and
+// hi in exact arithmetic: the float evaluation of xb is within a few ulp (< 0.01 px here) of it, and the
+// bound keeps half a pixel to spare.
+__device__ __forceinline__ bool window_inside(float lo, float hi, int width) {
+    return lo >= 0.5f && hi <= static_cast<float>(width) - 1.5f;
+}
+
+// The best score of a candidate sequence and its two neighbours, as the reference reads them from its
+// score array (stereo.cpp:181-199, 263-278): strict improvements only; the first best wins ties.
+struct PeakTracker {
+    float best = -2.0f, prev = -2.0f, before = -2.0f, after = -2.0f;
+    int best_k = -1;
+    __device__ __forceinline__ void push(int k, float sc) {
+        if (k == best_k + 1) after = sc;  // the score right after the current best
+        if (sc > best) {
+            best = sc;
+            best_k = k;
+            before = prev;
+            after = -3.0f;  // not yet known
+        }
+        prev = sc;
+    }
+};
 
 struct RefineArgs {
     const uint8_t* left;   // this level, w x h
@@ -114,7 +232,7 @@ struct RefineArgs {
 
 // refine_level (stereo.cpp:151-207): per pixel, ZNCC of slanted windows at 2x the coarse disparity +/-
 // search_radius in half-pixel steps; the best above min_zncc, with a parabola between its neighbours.
-static __global__ void __launch_bounds__(128) k_refine_level(RefineArgs a) {
+static __global__ void __launch_bounds__(128, 6) k_refine_level(RefineArgs a) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.w || y >= a.h) return;
     const size_t i = static_cast<size_t>(y) * a.w + x;
@@ -141,20 +259,33 @@ static __global__ void __launch_bounds__(128) k_refine_level(RefineArgs a) {
             const float center = __fmul_rn(2.0f, d0);
             const int nd = min(kMaxRefineCandidates, static_cast<int>(__fdiv_rn(static_cast<float>(2 * a.search_radius), kStep)) + 1);
             const float lo = __fsub_rn(center, static_cast<float>(a.search_radius));
-            float best = -2.0f, prev = -2.0f, before_best = -2.0f, after_best = -2.0f;
-            int best_k = -1;
-            for (int k = 0; k < nd; ++k) {
-                const float d = __fadd_rn(lo, __fmul_rn(kStep, static_cast<float>(k)));
-                const float sc = zncc_slanted(a.left, a.right, a.w, x, y, d, gx, gy, r);
-                if (k == best_k + 1) after_best = sc;  // the score right after the current best
-                if (sc > best) {
-                    best = sc;
-                    best_k = k;
-                    before_best = prev;
-                    after_best = -3.0f;  // not yet known
+            double sa, saa;
+            window_moments(a.left + static_cast<size_t>(y - r) * a.w + (x - r), a.w, 2 * r + 1, 2 * r + 1, sa, saa);
+            PeakTracker pk;
+            // Exact xb over the window and all candidates: x - d + u (1 - gx) - gy v, |u|, |v| <= r.
+            const float reach = __fadd_rn(__fmul_rn(static_cast<float>(r), __fsub_rn(1.0f, gx)),
+                                          __fmul_rn(static_cast<float>(r), fabsf(gy)));
+            const float fx = static_cast<float>(x), hi_d = __fadd_rn(lo, __fmul_rn(kStep, static_cast<float>(nd - 1)));
+            if (window_inside(__fsub_rn(__fsub_rn(fx, hi_d), reach), __fadd_rn(__fsub_rn(fx, lo), reach), a.w)) {
+                int k = 0;
+                for (; k + 1 < nd; k += 2) {
+                    const float2 d = f2(__fadd_rn(lo, __fmul_rn(kStep, static_cast<float>(k))),
+                                        __fadd_rn(lo, __fmul_rn(kStep, static_cast<float>(k + 1))));
+                    const float2 sc = zncc_slanted_pair(a.left, a.right, a.w, x, y, d, gx, gy, r, sa, saa);
+                    pk.push(k, sc.x);
+                    pk.push(k + 1, sc.y);
                 }
-                prev = sc;
+                if (k < nd)
+                    pk.push(k, zncc_slanted(a.left, a.right, a.w, x, y, __fadd_rn(lo, __fmul_rn(kStep, static_cast<float>(k))), gx,
+                                            gy, r, sa, saa));
+            } else {
+                for (int k = 0; k < nd; ++k) {
+                    const float d = __fadd_rn(lo, __fmul_rn(kStep, static_cast<float>(k)));
+                    pk.push(k, zncc_slanted(a.left, a.right, a.w, x, y, d, gx, gy, r, sa, saa));
+                }
             }
+            const float best = pk.best, before_best = pk.before, after_best = pk.after;
+            const int best_k = pk.best_k;
             bool keep = !(best_k < 0 || best < a.min_zncc);
             if (keep && a.reject_edge_winners && (best_k == 0 || best_k == nd - 1)) keep = false;
             if (keep) {
@@ -173,23 +304,48 @@ static __global__ void __launch_bounds__(128) k_refine_level(RefineArgs a) {
 
 // zncc_window (stereo.cpp:211-238).
 __device__ float zncc_window(const uint8_t* a, const uint8_t* b, int bw, int x0, int y0, int n, float cx, float cy, float D,
-                             float gx, float gy) {
+                             float gx, float gy, double sa, double saa) {
     ZnccSums s;
-    for (int j = 0; j < n; ++j) {
+    float fY = static_cast<float>(y0);
+    for (int j = 0; j < n; ++j, fY = __fadd_rn(fY, 1.0f)) {
         const int Y = y0 + j;
-        const uint8_t* ra = a + static_cast<size_t>(Y) * bw;
+        const uint8_t* ra = a + static_cast<size_t>(Y) * bw + x0;
         const uint8_t* rb = b + static_cast<size_t>(Y) * bw;
-        const float dy = __fmul_rn(gy, __fsub_rn(static_cast<float>(Y), cy));
-        for (int i = 0; i < n; ++i) {
-            const int X = x0 + i;
-            const float shift = __fadd_rn(__fadd_rn(D, __fmul_rn(gx, __fsub_rn(static_cast<float>(X), cx))), dy);
-            const float xb = __fsub_rn(static_cast<float>(X), shift);
+        const float dy = __fmul_rn(gy, __fsub_rn(fY, cy));
+        float fX = static_cast<float>(x0);
+        for (int i = 0; i < n; ++i, fX = __fadd_rn(fX, 1.0f)) {
+            const float shift = __fadd_rn(__fadd_rn(D, __fmul_rn(gx, __fsub_rn(fX, cx))), dy);
+            const float xb = __fsub_rn(fX, shift);
             double ib;
             if (!sample_row(rb, bw, xb, ib)) return kZnccNoWindow;
-            s.add(static_cast<double>(ra[X]), ib);
+            s.add(byte_to_double(ra[i]), ib);
         }
     }
-    return s.score(__dmul_rn(static_cast<double>(n), static_cast<double>(n)));
+    return s.score(sa, saa, __dmul_rn(static_cast<double>(n), static_cast<double>(n)));
+}
+
+// zncc_window for the disparities D.x and D.y (no range checks: see window_inside).
+__device__ float2 zncc_window_pair(const uint8_t* a, const uint8_t* b, int bw, int x0, int y0, int n, float cx, float cy, float2 D,
+                                   float gx, float gy, double sa, double saa) {
+    ZnccSums s0, s1;
+    float fY = static_cast<float>(y0);
+    for (int j = 0; j < n; ++j, fY = __fadd_rn(fY, 1.0f)) {
+        const int Y = y0 + j;
+        const uint8_t* ra = a + static_cast<size_t>(Y) * bw + x0;
+        const uint8_t* rb = b + static_cast<size_t>(Y) * bw;
+        const float dy = __fmul_rn(gy, __fsub_rn(fY, cy));
+        float fX = static_cast<float>(x0);
+        for (int i = 0; i < n; ++i, fX = __fadd_rn(fX, 1.0f)) {
+            const float gxx = __fmul_rn(gx, __fsub_rn(fX, cx));
+            const float2 shift = add2_rn(add2_rn(D, f2(gxx, gxx)), f2(dy, dy));
+            const float2 ib = bilinear_pair(rb, add2_rn(f2(fX, fX), neg2(shift)));
+            const double ia = byte_to_double(ra[i]);
+            s0.add(ia, static_cast<double>(ib.x));
+            s1.add(ia, static_cast<double>(ib.y));
+        }
+    }
+    const double m = __dmul_rn(static_cast<double>(n), static_cast<double>(n));
+    return f2(s0.score(sa, saa, m), s1.score(sa, saa, m));
 }
 
 struct DetailArgs {
@@ -212,7 +368,7 @@ __device__ __forceinline__ float detail_grad(float l, float c, float r) {
 
 // refine_detail (stereo.cpp:243-284): re-match each half-resolution disparity with a small full-resolution
 // window; keep the first estimate unless a clear peak lies inside the search.
-static __global__ void __launch_bounds__(128) k_refine_detail(DetailArgs a) {
+static __global__ void __launch_bounds__(128, 6) k_refine_detail(DetailArgs a) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= a.w || y >= a.h) return;
     const int n = 2 * a.radius, nc = 2 * a.K + 1;
@@ -225,20 +381,38 @@ static __global__ void __launch_bounds__(128) k_refine_detail(DetailArgs a) {
     const float gx = detail_grad(F(x - 1, y), d, F(x + 1, y)), gy = detail_grad(F(x, y - 1), d, F(x, y + 1));
     const float cx = __fadd_rn(__fmul_rn(2.0f, static_cast<float>(x)), 0.5f), cy = __fadd_rn(__fmul_rn(2.0f, static_cast<float>(y)), 0.5f);
     const float D0 = __fmul_rn(2.0f, d);
-    float best = -2.0f, prev = -2.0f, before_best = -2.0f, after_best = -2.0f;
-    int best_k = -1;
-    for (int k = 0; k < nc; ++k) {
-        const float D = __fadd_rn(D0, __fmul_rn(a.step, static_cast<float>(k - a.K)));
-        const float sc = zncc_window(a.full_left, a.full_right, a.W, x0, y0, n, cx, cy, D, gx, gy);
-        if (k == best_k + 1) after_best = sc;
-        if (sc > best) {
-            best = sc;
-            best_k = k;
-            before_best = prev;
-            after_best = -3.0f;
+    double sa, saa;
+    window_moments(a.full_left + static_cast<size_t>(y0) * a.W + x0, a.W, n, n, sa, saa);
+    PeakTracker pk;
+    // Exact xb over the window and all candidates: X (1 - gx) + gx cx - D - gy (Y - cy), X in [x0, x0 + n),
+    // Y in [y0, y0 + n), D within step * K of D0.
+    const float ax = __fmul_rn(fmaxf(fabsf(__fsub_rn(static_cast<float>(y0), cy)), fabsf(__fsub_rn(static_cast<float>(y0 + n - 1), cy))),
+                               fabsf(gy));
+    const float span = __fmul_rn(a.step, static_cast<float>(a.K));
+    const float base = __fmul_rn(gx, cx);
+    const float lo_x = __fsub_rn(__fsub_rn(__fadd_rn(__fmul_rn(static_cast<float>(x0), __fsub_rn(1.0f, gx)), base), __fadd_rn(D0, span)), ax);
+    const float hi_x = __fadd_rn(__fsub_rn(__fadd_rn(__fmul_rn(static_cast<float>(x0 + n - 1), __fsub_rn(1.0f, gx)), base),
+                                           __fsub_rn(D0, span)), ax);
+    if (window_inside(lo_x, hi_x, a.W)) {
+        int k = 0;
+        for (; k + 1 < nc; k += 2) {
+            const float2 D = f2(__fadd_rn(D0, __fmul_rn(a.step, static_cast<float>(k - a.K))),
+                                __fadd_rn(D0, __fmul_rn(a.step, static_cast<float>(k + 1 - a.K))));
+            const float2 sc = zncc_window_pair(a.full_left, a.full_right, a.W, x0, y0, n, cx, cy, D, gx, gy, sa, saa);
+            pk.push(k, sc.x);
+            pk.push(k + 1, sc.y);
         }
-        prev = sc;
+        if (k < nc)
+            pk.push(k, zncc_window(a.full_left, a.full_right, a.W, x0, y0, n, cx, cy,
+                                   __fadd_rn(D0, __fmul_rn(a.step, static_cast<float>(k - a.K))), gx, gy, sa, saa));
+    } else {
+        for (int k = 0; k < nc; ++k) {
+            const float D = __fadd_rn(D0, __fmul_rn(a.step, static_cast<float>(k - a.K)));
+            pk.push(k, zncc_window(a.full_left, a.full_right, a.W, x0, y0, n, cx, cy, D, gx, gy, sa, saa));
+        }
     }
+    const float best = pk.best, before_best = pk.before, after_best = pk.after;
+    const int best_k = pk.best_k;
     if (best_k <= 0 || best_k + 1 >= nc || best < a.min_zncc || before_best <= -2.0f || after_best <= -2.0f) return;
     float D = __fadd_rn(D0, __fmul_rn(a.step, static_cast<float>(best_k - a.K)));
     if (a.subpixel)
@@ -312,12 +486,14 @@ constexpr int kFindLimit = 1 << 22;
 
 // Root of x with path halving. Every parent index is at most its child's (roots are only ever hung under a
 // smaller root), so a halving store written concurrently with other finds or unions still names an
-// ancestor. Reads bypass L1 so that roots linked by other blocks are seen.
+// ancestor. While unions run (kLinking) reads bypass L1 so that roots linked by other blocks are seen;
+// afterwards roots no longer change and cached reads find them.
+template <bool kLinking>
 __device__ __forceinline__ int uf_find(int* parent, int x, int* err) {
     for (int it = 0; it < kFindLimit; ++it) {
-        const int p = __ldcg(parent + x);
+        const int p = kLinking ? __ldcg(parent + x) : parent[x];
         if (p == x) return x;
-        const int gp = __ldcg(parent + p);
+        const int gp = kLinking ? __ldcg(parent + p) : parent[p];
         if (gp != p) parent[x] = gp;
         x = gp;
     }
@@ -347,8 +523,8 @@ static __global__ void k_speckle_union(const float* __restrict__ disp, int w, in
         if (!valid_disparity(dj) || fabsf(__fsub_rn(dj, d)) > max_diff) continue;
         int a = i, b = j;
         for (int it = 0; it < kFindLimit; ++it) {
-            a = uf_find(parent, a, err);
-            b = uf_find(parent, b, err);
+            a = uf_find<true>(parent, a, err);
+            b = uf_find<true>(parent, b, err);
             if (a == b) break;
             if (a < b) {
                 const int t = a;
@@ -365,18 +541,22 @@ static __global__ void k_speckle_union(const float* __restrict__ disp, int w, in
 }
 
 // Component sizes once every union has landed. A find returns the true root however other threads halve
-// paths meanwhile, so the root is found again where it is used rather than stored in parent[].
+// paths meanwhile, so the root is found again where it is used rather than stored in parent[]. Lanes of a
+// warp with the same root add their count in one atomic (large regions would otherwise serialise on one
+// address).
 static __global__ void k_speckle_count(const float* __restrict__ disp, int n, int* parent, int* size, int* err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !valid_disparity(disp[i])) return;
-    atomicAdd(&size[uf_find(parent, i, err)], 1);
+    const bool act = i < n && valid_disparity(disp[i]);
+    const int r = act ? uf_find<false>(parent, i, err) : -1;
+    const unsigned same = __match_any_sync(0xFFFFFFFFu, r);
+    if (act && (__ffs(same) - 1) == static_cast<int>(threadIdx.x & 31)) atomicAdd(&size[r], __popc(same));
 }
 
 static __global__ void k_speckle_apply(float* __restrict__ disp, int n, int* parent, const int* __restrict__ size,
                                        int max_region_size, int* err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !valid_disparity(disp[i])) return;
-    if (size[uf_find(parent, i, err)] < max_region_size) disp[i] = kInvalid;
+    if (size[uf_find<false>(parent, i, err)] < max_region_size) disp[i] = kInvalid;
 }
 
 // The result's confidence is 0 wherever the disparity is invalid (stereo.cpp:531-533).
