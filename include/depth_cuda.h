@@ -295,6 +295,56 @@ DS_API int ds_disparity_to_points(const float* disparity, const float* confidenc
 DS_API int ds_pack_depth(const float* points_xyzw, const float* weights, int width, int height, uint8_t* packed,
                          void* stream);
 
+/* ---- Marker blob search on the raw images -------------------------------------------------------------
+ * depth_metal::BlobParams / BlobBox (metal_stereo.hpp:21-39) and MetalStereo::set_blob_params /
+ * FrameRequest::marker_blobs (metal_stereo.hpp:41-58, 94-95): connected pixels above `threshold`
+ * (4-neighbourhood, markers::find_blobs, libs/markers/src/detect.cpp:14-45), gated by box size, aspect,
+ * fill and border, then a dark-ring pre-check on the blob's moment ellipse (the reference's GPU search,
+ * stereo_kernels.metal.inc:770-901). The ring test uses exact half-angle formulas and a table of the 16
+ * ring directions instead of atan2/cos/sin, so candidates are reproducible bit for bit. Candidates come
+ * back ordered by their first pixel in raster order (the order of the CPU detector); when more than
+ * max_blobs pass, `found` counts them all and which max_blobs are kept is unspecified. */
+typedef struct ds_blob_params {
+    uint32_t threshold;      /* 150: grey level a blob pixel exceeds */
+    uint32_t min_diameter;   /* 3: box width and height limits (px) */
+    uint32_t max_diameter;   /* 60 */
+    float max_aspect;        /* 4: box aspect */
+    float min_fill;          /* 0.5: pixels / (box area * pi / 4) */
+    uint32_t border;         /* 4: room for the background ring */
+    float max_axis_ratio;    /* 3: moment-ellipse axis ratio (x 1.2 leeway) */
+    float ring_scale;        /* 1.4: the dark ring at this multiple of the moment ellipse */
+    float ring_contrast;     /* 0.5: ring level between background and peak */
+    float ring_max_bright;   /* 0.3: fraction of the 16 ring samples allowed above that level */
+    uint32_t max_blobs;      /* 1024: candidates returned per image (1..65536) */
+} ds_blob_params;
+
+typedef struct ds_blob_box {
+    uint32_t x0, y0, x1, y1; /* inclusive box */
+    uint32_t pixels, peak;
+} ds_blob_box;
+
+/* Candidates of both raw images of a frame; `left`/`right` hold `capacity` boxes each (host memory). */
+typedef struct ds_blob_boxes {
+    ds_blob_box* left;
+    ds_blob_box* right;
+    uint32_t capacity;
+    uint32_t found[2];       /* out: candidates that passed (before any cap) */
+    uint32_t kept[2];        /* out: boxes written */
+} ds_blob_boxes;
+
+DS_API void ds_default_blob_params(ds_blob_params* params);
+/* MetalStereo::set_blob_params: enables the blob search of ds_compute_raw_blobs; buffers are sized on
+ * first use. */
+DS_API int ds_set_blob_params(ds_handle* handle, const ds_blob_params* params);
+/* ds_compute_raw plus the blob search on both raw images, run on a second stream concurrently with the
+ * stereo (MetalStereo::compute_frame with FrameRequest::marker_blobs). */
+DS_API int ds_compute_raw_blobs(ds_handle* handle, const uint8_t* raw_left, const uint8_t* raw_right, ptrdiff_t stride,
+                                const ds_outputs* out, ds_blob_boxes* blobs);
+/* The blob search alone on one host image of any size (width x height, rows `stride` bytes apart):
+ * up to `capacity` boxes, `found` = candidates that passed. Needs ds_set_blob_params. */
+DS_API int ds_find_blobs(ds_handle* handle, const uint8_t* image, int width, int height, ptrdiff_t stride, ds_blob_box* out,
+                         uint32_t capacity, uint32_t* found, uint32_t* kept);
+
 /* ---- Request server: continuous batching of frames as they arrive (no counterpart in the reference,
  * whose frontend runs one camera pair synchronously, libs/pipeline/src/stereo_frontend.cpp:302-330) ------
  * A worker thread admits submitted frames in arrival order as soon as a slot (a CUDA stream with its own

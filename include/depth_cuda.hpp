@@ -7,6 +7,7 @@
 // Header-only; link with libdepth_cuda.so. Requires C++23 (std::expected, as the reference).
 #pragma once
 
+#include <array>
 #include <cstddef>
 #include <cstdint>
 #include <expected>
@@ -91,6 +92,21 @@ struct StereoParams {
     float speckle_max_diff = 1.0f;
 };
 
+// depth_metal::BlobParams / BlobBox (libs/depth_metal/include/einstar/depth_metal/metal_stereo.hpp:21-39).
+struct BlobParams {
+    std::uint32_t threshold = 150;
+    std::uint32_t min_diameter = 3, max_diameter = 60;
+    float max_aspect = 4.0f;
+    float min_fill = 0.5f;
+    std::uint32_t border = 4;
+    float max_axis_ratio = 3.0f;
+    float ring_scale = 1.4f;
+    float ring_contrast = 0.5f;
+    float ring_max_bright = 0.3f;
+    std::uint32_t max_blobs = 1024;
+};
+using BlobBox = ds_blob_box;
+
 // depth::RectifiedGeometry (libs/depth/include/einstar/depth/point_image.hpp:12-26).
 struct RectifiedGeometry {
     double f = 0, cx = 0, cy = 0, baseline = 0, cx_offset = 0;
@@ -120,6 +136,10 @@ struct StereoResult {
     std::vector<float> disparity, confidence;
     std::vector<std::uint16_t> disparity_u16;
     std::vector<float> depth;
+    // compute_raw with marker blobs: candidates of the left and right raw images and how many passed
+    // (depth_metal::FrameOutputs::blobs / blobs_found).
+    std::array<std::vector<BlobBox>, 2> blobs;
+    std::array<std::uint32_t, 2> blobs_found{};
 };
 
 class CudaStereo {
@@ -157,6 +177,31 @@ public:
     Result<StereoResult> compute_raw(ImageViewU8 raw_left, ImageViewU8 raw_right, std::vector<std::uint8_t>* rect_left = nullptr,
                                      std::vector<std::uint8_t>* rect_right = nullptr) {
         return run(raw_left, raw_right, true, rect_left, rect_right);
+    }
+
+    // MetalStereo::set_blob_params: enables compute_raw(..., marker_blobs = true) and find_blobs.
+    Result<void> set_blob_params(const BlobParams& p) {
+        const ds_blob_params c{p.threshold, p.min_diameter, p.max_diameter, p.max_aspect, p.min_fill, p.border,
+                               p.max_axis_ratio, p.ring_scale, p.ring_contrast, p.ring_max_bright, p.max_blobs};
+        if (auto r = check(ds_set_blob_params(h_, &c)); !r) return r;
+        max_blobs_ = p.max_blobs;
+        return {};
+    }
+
+    // Raw pair -> stereo, with the marker blob search on both raw images (FrameRequest::marker_blobs).
+    Result<StereoResult> compute_raw_blobs(ImageViewU8 raw_left, ImageViewU8 raw_right) {
+        return run(raw_left, raw_right, true, nullptr, nullptr, true);
+    }
+
+    // The blob search alone on one image: candidates ordered by first pixel.
+    Result<std::vector<BlobBox>> find_blobs(ImageViewU8 img, std::uint32_t* found = nullptr) {
+        std::vector<BlobBox> out(max_blobs_);
+        std::uint32_t f = 0, k = 0;
+        if (auto r = check(ds_find_blobs(h_, img.data, img.width, img.height, img.stride, out.data(), max_blobs_, &f, &k)); !r)
+            return std::unexpected(r.error());
+        out.resize(k);
+        if (found) *found = f;
+        return out;
     }
 
     const StereoTimings& last_timings() {
@@ -202,7 +247,7 @@ private:
     }
 
     Result<StereoResult> run(ImageViewU8 l, ImageViewU8 r, bool raw, std::vector<std::uint8_t>* rl,
-                             std::vector<std::uint8_t>* rr) {
+                             std::vector<std::uint8_t>* rr, bool blobs = false) {
         if (!l.data || !r.data) return std::unexpected(Error{Errc::invalid_argument, "null image"});
         if (l.stride != r.stride || l.width != r.width || l.height != r.height)
             return std::unexpected(Error{Errc::invalid_argument, "left and right images differ in size or stride"});
@@ -220,7 +265,18 @@ private:
         if (rr) rr->resize(n);
         ds_outputs o{res.disparity.data(), res.confidence.data(), res.disparity_u16.data(),
                      have_points_ ? res.depth.data() : nullptr, rl ? rl->data() : nullptr, rr ? rr->data() : nullptr};
-        const int rc = raw ? ds_compute_raw(h_, l.data, r.data, l.stride, &o) : ds_compute(h_, l.data, r.data, l.stride, &o);
+        int rc = DS_OK;
+        if (blobs) {
+            res.blobs[0].resize(max_blobs_);
+            res.blobs[1].resize(max_blobs_);
+            ds_blob_boxes bb{res.blobs[0].data(), res.blobs[1].data(), max_blobs_, {0, 0}, {0, 0}};
+            rc = ds_compute_raw_blobs(h_, l.data, r.data, l.stride, &o, &bb);
+            res.blobs[0].resize(bb.kept[0]);
+            res.blobs[1].resize(bb.kept[1]);
+            res.blobs_found = {bb.found[0], bb.found[1]};
+        } else {
+            rc = raw ? ds_compute_raw(h_, l.data, r.data, l.stride, &o) : ds_compute(h_, l.data, r.data, l.stride, &o);
+        }
         if (rc != DS_OK) return std::unexpected(Error{static_cast<Errc>(rc), ds_last_error(h_)});
         return res;
     }
@@ -228,6 +284,7 @@ private:
     ds_handle* h_;
     int w_, h_px_;
     bool have_points_ = false;
+    std::uint32_t max_blobs_ = 1024;
     StereoTimings timings_;
 };
 

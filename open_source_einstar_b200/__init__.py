@@ -5,7 +5,9 @@ depth, as hand-written sm_100a CUDA behind the C ABI in include/depth_cuda.h (li
 The Python classes mirror the reference's stereo-matcher interface (depth_metal::MetalStereo).
 """
 from .stereo import (  # noqa: F401
+    BLOB_FIELDS,
     INVALID_DISPARITY,
+    BlobParams,
     CudaStereo,
     DetailParams,
     Errc,

@@ -68,6 +68,18 @@ class PointParamsC(C.Structure):
                 ("edge_weight", C.c_float), ("weight_reference_depth_mm", C.c_float)]
 
 
+class BlobParamsC(C.Structure):
+    _fields_ = [("threshold", C.c_uint32), ("min_diameter", C.c_uint32), ("max_diameter", C.c_uint32),
+                ("max_aspect", C.c_float), ("min_fill", C.c_float), ("border", C.c_uint32), ("max_axis_ratio", C.c_float),
+                ("ring_scale", C.c_float), ("ring_contrast", C.c_float), ("ring_max_bright", C.c_float),
+                ("max_blobs", C.c_uint32)]
+
+
+class BlobBoxesC(C.Structure):
+    _fields_ = [("left", C.c_void_p), ("right", C.c_void_p), ("capacity", C.c_uint32), ("found", C.c_uint32 * 2),
+                ("kept", C.c_uint32 * 2)]
+
+
 class ServerOptionsC(C.Structure):
     _fields_ = [("volume_budget_bytes", C.c_size_t), ("max_slots", C.c_int), ("max_pending", C.c_int)]
 
@@ -127,6 +139,10 @@ SIGNATURES = {
     "ds_default_point_params": (None, [C.POINTER(PointParamsC)]),
     "ds_disparity_to_points": (_i, [_vp, _vp, _i, _i, C.POINTER(GeometryC), C.POINTER(PointParamsC), _vp, _vp, _vp, _vp]),
     "ds_pack_depth": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
+    "ds_default_blob_params": (None, [C.POINTER(BlobParamsC)]),
+    "ds_set_blob_params": (_i, [_vp, C.POINTER(BlobParamsC)]),
+    "ds_compute_raw_blobs": (_i, [_vp, _vp, _vp, C.c_ssize_t, C.POINTER(OutputsC), C.POINTER(BlobBoxesC)]),
+    "ds_find_blobs": (_i, [_vp, _vp, _i, _i, C.c_ssize_t, _vp, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "ds_server_create": (_i, [C.POINTER(ServerOptionsC), C.POINTER(_vp)]),
     "ds_server_destroy": (None, [_vp]),
     "ds_server_last_error": (C.c_char_p, [_vp]),

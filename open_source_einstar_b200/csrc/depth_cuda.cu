@@ -19,6 +19,7 @@
 #include "fused_kernels.cuh"
 #include "internal.h"
 #include "refine_kernels.cuh"
+#include "blob_kernels.cuh"
 
 namespace {
 
@@ -117,6 +118,23 @@ struct ds_handle {
     int* d_size = nullptr;
     int* d_err = nullptr;
 
+    // Marker blob search (ds_set_blob_params), one set of buffers per side, sized for blob_px pixels.
+    bool have_blobs = false;
+    ds_blob_params blob_p{};
+    size_t blob_px = 0;
+    struct BlobBufs {
+        int* parent = nullptr;
+        uint32_t* count = nullptr;
+        uint32_t* box = nullptr;
+        int* mom = nullptr;
+        dsk::BlobCand* out = nullptr;
+        uint32_t* n_out = nullptr;  // [0] candidates found, [1] error flag
+        uint8_t* img = nullptr;     // a host image's upload (ds_find_blobs)
+    } blob[2];
+    uint32_t blob_cap = 0;
+    cudaStream_t blob_stream = nullptr;
+    cudaEvent_t blob_ev = nullptr;
+
     ds_geometry geom{};
     float min_depth = 150.0f, max_depth = 700.0f, max_jump = 4.0f;
     bool have_points = false;
@@ -171,6 +189,17 @@ void release(ds_handle* h) {
     f(h->d_parent);
     f(h->d_size);
     f(h->d_err);
+    for (auto& b : h->blob) {
+        f(b.parent);
+        f(b.count);
+        f(b.box);
+        f(b.mom);
+        f(b.out);
+        f(b.n_out);
+        f(b.img);
+    }
+    if (h->blob_ev) cudaEventDestroy(h->blob_ev);
+    if (h->blob_stream) cudaStreamDestroy(h->blob_stream);
     if (h->sgm) {
         release(h->sgm);
         delete h->sgm;
@@ -649,7 +678,95 @@ ds_outputs internal_outputs(ds_handle* h) {
     return o;
 }
 
-int run_host(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t stride, const ds_outputs* out, bool raw) {
+// ---- marker blob search -------------------------------------------------------------------------------------
+void ensure_blob_buffers(ds_handle* h, size_t npx) {
+    const uint32_t cap = h->blob_p.max_blobs;
+    if (npx <= h->blob_px && cap == h->blob_cap) return;
+    npx = std::max(npx, h->blob_px);
+    for (auto& b : h->blob) {
+        for (void* q : {static_cast<void*>(b.parent), static_cast<void*>(b.count), static_cast<void*>(b.box), static_cast<void*>(b.mom),
+                        static_cast<void*>(b.out), static_cast<void*>(b.n_out), static_cast<void*>(b.img)})
+            if (q) cudaFree(q);
+        b = ds_handle::BlobBufs{};
+        b.parent = h->alloc<int>(npx);
+        b.count = h->alloc<uint32_t>(npx);
+        b.box = h->alloc<uint32_t>(5 * npx);
+        b.mom = h->alloc<int>(5 * npx);
+        b.out = h->alloc<dsk::BlobCand>(cap);
+        b.n_out = h->alloc<uint32_t>(2);
+        b.img = h->alloc<uint8_t>(npx);
+    }
+    h->blob_px = npx;
+    h->blob_cap = cap;
+    if (!h->blob_stream) {
+        DS_CUDA(cudaStreamCreateWithFlags(&h->blob_stream, cudaStreamNonBlocking));
+        DS_CUDA(cudaEventCreateWithFlags(&h->blob_ev, cudaEventDisableTiming));
+    }
+}
+
+// The blob search of one image (w x h, tightly packed, on the device) into side `side`'s candidate list.
+void enqueue_blob_search(ds_handle* h, int side, const uint8_t* img, int w, int ht, cudaStream_t st) {
+    auto& b = h->blob[side];
+    const auto& bp = h->blob_p;
+    dsk::BlobArgs a{};
+    a.img = img;
+    a.w = w;
+    a.h = ht;
+    a.threshold = bp.threshold;
+    a.min_diameter = bp.min_diameter;
+    a.max_diameter = bp.max_diameter;
+    a.border = bp.border;
+    a.max_out = h->blob_cap;
+    a.max_aspect = bp.max_aspect;
+    a.min_fill = bp.min_fill;
+    a.max_axis_ratio = bp.max_axis_ratio;
+    a.ring_scale = bp.ring_scale;
+    a.ring_contrast = bp.ring_contrast;
+    a.ring_max_bright = bp.ring_max_bright;
+    a.parent = b.parent;
+    a.count = b.count;
+    a.box = b.box;
+    a.mom = b.mom;
+    a.out = b.out;
+    a.n_out = b.n_out;
+    a.err = reinterpret_cast<int*>(b.n_out + 1);
+    DS_CUDA(cudaMemsetAsync(b.n_out, 0, 2 * sizeof(uint32_t), st));
+    const int n = w * ht, bl = (n + 255) / 256;
+    dsk::k_blob_init<<<bl, 256, 0, st>>>(a);
+    dsk::k_blob_union<<<dim3((w + 31) / 32, (ht + 7) / 8), dim3(32, 8), 0, st>>>(a);
+    dsk::k_blob_stats<<<bl, 256, 0, st>>>(a);
+    dsk::k_blob_select<<<bl, 256, 0, st>>>(a);
+    g_launches += 4;
+    DS_CUDA(cudaGetLastError());
+}
+
+// Host side of a search: the found count, the error flag and the candidate list, read back on `st`.
+struct BlobHost {
+    std::vector<dsk::BlobCand> cand;
+    uint32_t head[2] = {0, 0};
+};
+
+void blob_readback(ds_handle* h, int side, BlobHost& hb, cudaStream_t st) {
+    hb.cand.resize(h->blob_cap);
+    DS_CUDA(cudaMemcpyAsync(hb.head, h->blob[side].n_out, sizeof(hb.head), cudaMemcpyDeviceToHost, st));
+    DS_CUDA(cudaMemcpyAsync(hb.cand.data(), h->blob[side].out, h->blob_cap * sizeof(dsk::BlobCand), cudaMemcpyDeviceToHost, st));
+}
+
+// After the stream has finished: candidates ordered by first pixel, at most `capacity` written.
+int blob_finish(ds_handle* h, const BlobHost& hb, ds_blob_box* out, uint32_t capacity, uint32_t* found, uint32_t* kept) {
+    if (hb.head[1]) return h->fail(DS_IO, "blob search: union-find exceeded its iteration bound");
+    const uint32_t n = std::min(hb.head[0], h->blob_cap);
+    std::vector<dsk::BlobCand> c(hb.cand.begin(), hb.cand.begin() + n);
+    std::sort(c.begin(), c.end(), [](const dsk::BlobCand& p, const dsk::BlobCand& q) { return p.root < q.root; });
+    const uint32_t k = std::min(n, capacity);
+    for (uint32_t i = 0; i < k; ++i) out[i] = ds_blob_box{c[i].x0, c[i].y0, c[i].x1, c[i].y1, c[i].pixels, c[i].peak};
+    if (found) *found = hb.head[0];
+    if (kept) *kept = k;
+    return DS_OK;
+}
+
+int run_host(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t stride, const ds_outputs* out, bool raw,
+             ds_blob_boxes* blobs = nullptr) {
     const double t0 = now_ms();
     const int iw = raw ? h->raw_w : h->w, ih = raw ? h->raw_h : h->h;
     if (!left || !right) return h->fail(DS_INVALID_ARGUMENT, "null image");
@@ -660,6 +777,16 @@ int run_host(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t 
     for (int s = 0; s < 2; ++s)
         DS_CUDA(cudaMemcpy2DAsync(dst[s], iw, src[s], stride, iw, ih, cudaMemcpyHostToDevice, h->stream));
     DS_CUDA(cudaEventRecord(h->ev0, h->stream));
+    BlobHost bh[2];
+    if (blobs) {  // on the raw images, concurrently with the stereo
+        ensure_blob_buffers(h, static_cast<size_t>(iw) * ih);
+        DS_CUDA(cudaEventRecord(h->blob_ev, h->stream));
+        DS_CUDA(cudaStreamWaitEvent(h->blob_stream, h->blob_ev, 0));
+        for (int s = 0; s < 2; ++s) {
+            enqueue_blob_search(h, s, dst[s], iw, ih, h->blob_stream);
+            blob_readback(h, s, bh[s], h->blob_stream);
+        }
+    }
     enqueue_frame(h, dst[0], dst[1], raw, internal_outputs(h), h->stream);
     DS_CUDA(cudaEventRecord(h->ev1, h->stream));
     const size_t n = static_cast<size_t>(h->w) * h->h;
@@ -672,6 +799,12 @@ int run_host(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t 
         if (out->rect_right) DS_CUDA(cudaMemcpyAsync(out->rect_right, h->d_rect[1], n, cudaMemcpyDeviceToHost, h->stream));
     }
     DS_CUDA(cudaStreamSynchronize(h->stream));
+    if (blobs) {
+        DS_CUDA(cudaStreamSynchronize(h->blob_stream));
+        ds_blob_box* bo[2] = {blobs->left, blobs->right};
+        for (int s = 0; s < 2; ++s)
+            if (const int rc = blob_finish(h, bh[s], bo[s], blobs->capacity, &blobs->found[s], &blobs->kept[s]); rc != DS_OK) return rc;
+    }
     if (h->refine && h->p.speckle_max_region_size > 1) {
         int err = 0;
         DS_CUDA(cudaMemcpy(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1136,6 +1269,50 @@ DS_API int ds_compute_raw(ds_handle* h, const uint8_t* left, const uint8_t* righ
     if (!h) return DS_INVALID_ARGUMENT;
     if (!h->have_rect) return h->fail(DS_INVALID_ARGUMENT, "set_rectification() not called");
     return guarded(h, [&] { return run_host(h, left, right, stride, out, true); });
+}
+
+DS_API void ds_default_blob_params(ds_blob_params* p) {
+    if (!p) return;
+    *p = ds_blob_params{150u, 3u, 60u, 4.0f, 0.5f, 4u, 3.0f, 1.4f, 0.5f, 0.3f, 1024u};  // depth_metal::BlobParams
+}
+
+DS_API int ds_set_blob_params(ds_handle* h, const ds_blob_params* p) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    if (!p) return h->fail(DS_INVALID_ARGUMENT, "null blob parameters");
+    if (p->max_blobs < 1 || p->max_blobs > 65536) return h->fail(DS_INVALID_ARGUMENT, "max_blobs must be 1..65536");
+    if (p->min_diameter > p->max_diameter || p->threshold > 255)
+        return h->fail(DS_INVALID_ARGUMENT, "blob parameters: threshold 0..255 and min_diameter <= max_diameter");
+    h->blob_p = *p;
+    h->have_blobs = true;
+    return DS_OK;
+}
+
+DS_API int ds_compute_raw_blobs(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t stride, const ds_outputs* out,
+                                ds_blob_boxes* blobs) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    if (!h->have_rect) return h->fail(DS_INVALID_ARGUMENT, "set_rectification() not called");
+    if (!blobs || !blobs->left || !blobs->right) return h->fail(DS_INVALID_ARGUMENT, "null blob outputs");
+    if (!h->have_blobs) return h->fail(DS_INVALID_ARGUMENT, "set_blob_params() not called");
+    return guarded(h, [&] { return run_host(h, left, right, stride, out, true, blobs); });
+}
+
+DS_API int ds_find_blobs(ds_handle* h, const uint8_t* image, int width, int height, ptrdiff_t stride, ds_blob_box* out,
+                         uint32_t capacity, uint32_t* found, uint32_t* kept) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    if (!image || (!out && capacity > 0)) return h->fail(DS_INVALID_ARGUMENT, "null image or output");
+    if (!h->have_blobs) return h->fail(DS_INVALID_ARGUMENT, "set_blob_params() not called");
+    if (width < 1 || height < 1 || width > 16384 || height > 16384) return h->fail(DS_INVALID_ARGUMENT, "image size must be 1..16384");
+    if (stride < width) return h->fail(DS_INVALID_ARGUMENT, "stride smaller than the image width");
+    return guarded(h, [&]() -> int {
+        ensure_blob_buffers(h, static_cast<size_t>(width) * height);
+        cudaStream_t st = h->blob_stream;
+        DS_CUDA(cudaMemcpy2DAsync(h->blob[0].img, width, image, stride, width, height, cudaMemcpyHostToDevice, st));
+        enqueue_blob_search(h, 0, h->blob[0].img, width, height, st);
+        BlobHost bh;
+        blob_readback(h, 0, bh, st);
+        DS_CUDA(cudaStreamSynchronize(st));
+        return blob_finish(h, bh, out, capacity, found, kept);
+    });
 }
 
 static int run_device(ds_handle* h, const uint8_t* left, const uint8_t* right, const ds_outputs* out, void* stream, bool raw) {

@@ -8,6 +8,7 @@
 #include <cstdint>
 
 #include "stereo_kernels.cuh"
+#include "union_find.cuh"
 
 namespace dsk {
 
@@ -481,26 +482,6 @@ static __global__ void k_filter_spikes(const float* __restrict__ in, int w, int 
 // ---- speckle removal (stereo.cpp:465-494) as connected components by union-find -------------------------
 // Regions are connected under |d_a - d_b| <= max_diff between 4-neighbours, which is symmetric, so the
 // components (and therefore the removed pixels) do not depend on the order the reference visits them.
-// Every loop here is bounded; a bound that runs out sets *err.
-constexpr int kFindLimit = 1 << 22;
-
-// Root of x with path halving. Every parent index is at most its child's (roots are only ever hung under a
-// smaller root), so a halving store written concurrently with other finds or unions still names an
-// ancestor. While unions run (kLinking) reads bypass L1 so that roots linked by other blocks are seen;
-// afterwards roots no longer change and cached reads find them.
-template <bool kLinking>
-__device__ __forceinline__ int uf_find(int* parent, int x, int* err) {
-    for (int it = 0; it < kFindLimit; ++it) {
-        const int p = kLinking ? __ldcg(parent + x) : parent[x];
-        if (p == x) return x;
-        const int gp = kLinking ? __ldcg(parent + p) : parent[p];
-        if (gp != p) parent[x] = gp;
-        x = gp;
-    }
-    *err = 1;
-    return x;
-}
-
 static __global__ void k_speckle_init(const float* __restrict__ disp, int n, int* __restrict__ parent, int* __restrict__ size) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -521,22 +502,7 @@ static __global__ void k_speckle_union(const float* __restrict__ disp, int w, in
         if (j < 0) continue;
         const float dj = disp[j];
         if (!valid_disparity(dj) || fabsf(__fsub_rn(dj, d)) > max_diff) continue;
-        int a = i, b = j;
-        for (int it = 0; it < kFindLimit; ++it) {
-            a = uf_find<true>(parent, a, err);
-            b = uf_find<true>(parent, b, err);
-            if (a == b) break;
-            if (a < b) {
-                const int t = a;
-                a = b;
-                b = t;
-            }
-            // a > b: hang root a under b unless another thread changed a's parent first
-            const int old = atomicCAS(&parent[a], a, b);
-            if (old == a) break;
-            a = old;
-            if (it + 1 == kFindLimit) *err = 1;
-        }
+        uf_union(parent, i, j, err);
     }
 }
 

@@ -165,6 +165,34 @@ class StereoResult:
     depth: np.ndarray | None = None
     rect_left: np.ndarray | None = None
     rect_right: np.ndarray | None = None
+    # compute_raw(blobs=True): candidate boxes (x0, y0, x1, y1, pixels, peak) of the left and right raw
+    # images, and how many passed before the max_blobs cap (depth_metal::FrameOutputs::blobs / blobs_found)
+    blobs: tuple | None = None
+    blobs_found: tuple | None = None
+
+
+@dataclass
+class BlobParams:
+    """depth_metal::BlobParams (libs/depth_metal/include/einstar/depth_metal/metal_stereo.hpp:21-35)."""
+    threshold: int = 150
+    min_diameter: int = 3
+    max_diameter: int = 60
+    max_aspect: float = 4.0
+    min_fill: float = 0.5
+    border: int = 4
+    max_axis_ratio: float = 3.0
+    ring_scale: float = 1.4
+    ring_contrast: float = 0.5
+    ring_max_bright: float = 0.3
+    max_blobs: int = 1024
+
+    def c(self) -> N.BlobParamsC:
+        return N.BlobParamsC(int(self.threshold), int(self.min_diameter), int(self.max_diameter), float(self.max_aspect),
+                             float(self.min_fill), int(self.border), float(self.max_axis_ratio), float(self.ring_scale),
+                             float(self.ring_contrast), float(self.ring_max_bright), int(self.max_blobs))
+
+
+BLOB_FIELDS = ("x0", "y0", "x1", "y1", "pixels", "peak")
 
 
 def _ptr(a) -> int | None:
@@ -197,6 +225,7 @@ class CudaStereo:
         self.height = height
         self.raw_size: tuple[int, int] | None = None
         self.geometry: RectifiedGeometry | None = None
+        self.blob_params: BlobParams | None = None
 
     # --- life cycle ---------------------------------------------------------------------------------
     @classmethod
@@ -284,10 +313,12 @@ class CudaStereo:
         return res
 
     def compute_raw(self, raw_left: np.ndarray, raw_right: np.ndarray, rectified: bool = False,
-                    out: StereoResult | None = None) -> StereoResult:
+                    out: StereoResult | None = None, blobs: bool = False) -> StereoResult:
         """MetalStereo::compute_raw (metal_stereo.cpp:340-349): rectify on the device, then stereo. With
         `rectified`, the rectified pair is returned too (the rect_left / rect_right out-parameters).
-        `out` may hold preallocated host arrays (None entries are not produced)."""
+        `out` may hold preallocated host arrays (None entries are not produced). With `blobs`, the marker
+        blob search runs on both raw images concurrently (FrameRequest::marker_blobs; set_blob_params first)
+        and res.blobs holds the candidates, (k, 6) uint32 arrays of BLOB_FIELDS."""
         if self.raw_size is None:
             raise StereoError(Errc.invalid_argument, "set_rectification() not called")
         rw, rh = self.raw_size
@@ -296,9 +327,43 @@ class CudaStereo:
         if raw_left.strides[0] != raw_right.strides[0]:
             raw_left, raw_right = np.ascontiguousarray(raw_left), np.ascontiguousarray(raw_right)
         res, o = (out, self._outputs_of(out)) if out is not None else self._outputs(rectified)
-        self._check(N.lib().ds_compute_raw(self._h, raw_left.ctypes.data, raw_right.ctypes.data, raw_left.strides[0],
-                                           C.byref(o)))
+        if not blobs:
+            self._check(N.lib().ds_compute_raw(self._h, raw_left.ctypes.data, raw_right.ctypes.data, raw_left.strides[0],
+                                               C.byref(o)))
+            return res
+        if self.blob_params is None:
+            raise StereoError(Errc.invalid_argument, "set_blob_params() not called")
+        cap = self.blob_params.max_blobs
+        bl, br = np.zeros((cap, 6), np.uint32), np.zeros((cap, 6), np.uint32)
+        bb = N.BlobBoxesC(bl.ctypes.data, br.ctypes.data, cap)
+        self._check(N.lib().ds_compute_raw_blobs(self._h, raw_left.ctypes.data, raw_right.ctypes.data, raw_left.strides[0],
+                                                 C.byref(o), C.byref(bb)))
+        res.blobs = (bl[:bb.kept[0]].copy(), br[:bb.kept[1]].copy())
+        res.blobs_found = (int(bb.found[0]), int(bb.found[1]))
         return res
+
+    def set_blob_params(self, params: "BlobParams | None" = None) -> None:
+        """MetalStereo::set_blob_params (metal_stereo.cpp:279-291)."""
+        params = params or BlobParams()
+        self._check(N.lib().ds_set_blob_params(self._h, C.byref(params.c())))
+        self.blob_params = params
+
+    def find_blobs(self, image: np.ndarray) -> tuple[np.ndarray, int]:
+        """The marker blob search alone on one host image: ((k, 6) uint32 candidates of BLOB_FIELDS ordered
+        by first pixel, number that passed before the max_blobs cap)."""
+        if self.blob_params is None:
+            raise StereoError(Errc.invalid_argument, "set_blob_params() not called")
+        img = np.asarray(image)
+        if img.dtype != np.uint8 or img.ndim != 2:
+            raise StereoError(Errc.invalid_argument, "blob image must be a 2-D uint8 array")
+        if img.strides[1] != 1:
+            img = np.ascontiguousarray(img)
+        cap = self.blob_params.max_blobs
+        out = np.zeros((cap, 6), np.uint32)
+        found, kept = C.c_uint32(), C.c_uint32()
+        self._check(N.lib().ds_find_blobs(self._h, img.ctypes.data, img.shape[1], img.shape[0], img.strides[0], out.ctypes.data,
+                                          cap, C.byref(found), C.byref(kept)))
+        return out[:kept.value].copy(), int(found.value)
 
     def compute_device(self, left, right, outputs: dict, stream=None, raw: bool = False) -> None:
         """Device-resident frame: `left`/`right` and every tensor in `outputs` (keys of ds_outputs:

@@ -545,3 +545,65 @@ def recording_frame(rec: Recording, i: int, device="cpu") -> tuple[np.ndarray, n
     left, _ = render(scene, rig.left, R_wl, tuple(c_l), seed=7 * i + 1, device=device)
     right, _ = render(scene, rig.right, R_wr, tuple(c_r), seed=7 * i + 2, device=device)
     return left, right
+
+
+@dataclass
+class MarkerLayout:
+    """Stickers and distractors composited into an IR image (pixel coordinates)."""
+    markers: list  # (cx, cy, a, b, angle): white disc semi-axes a >= b, angle of a
+    glints: list   # (cx, cy, r): bright spots on a bright surround
+    dots: list     # (cx, cy): small bright speckle-like dots
+
+
+def add_markers(img: np.ndarray, n_markers: int = 20, seed: int = 0, radius=(3.0, 9.0), n_glints: int = 6, n_dots: int = 40,
+                margin: int = 24) -> tuple[np.ndarray, MarkerLayout]:
+    """Composites retro-reflective marker stickers into an 8-bit IR image, as the scanner sees them under its
+    ring light: a saturated elliptical disc (a foreshortened circle) inside a dark ring of 1.8x its size,
+    sigma 2 DN noise. Distractors: bright glints on a bright surround and small bright dots. Stickers do
+    not overlap; every one lies at least `margin` pixels inside the image."""
+    rng = np.random.default_rng(30_000 + seed)
+    out = np.array(img, dtype=np.float32, copy=True)
+    h, w = out.shape
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float32)
+    placed = []
+
+    def free(cx, cy, r):
+        return all((cx - px) ** 2 + (cy - py) ** 2 > (r + pr + 4) ** 2 for px, py, pr in placed)
+
+    markers, glints, dots = [], [], []
+    tries = 0
+    while len(markers) < n_markers and tries < 50 * n_markers:
+        tries += 1
+        a = float(rng.uniform(*radius))
+        b = a * float(rng.uniform(0.45, 1.0))
+        ang = float(rng.uniform(0, math.pi))
+        cx, cy = float(rng.uniform(margin + 2 * a, w - margin - 2 * a)), float(rng.uniform(margin + 2 * a, h - margin - 2 * a))
+        if not free(cx, cy, 2.0 * a):
+            continue
+        placed.append((cx, cy, 2.0 * a))
+        c, s = math.cos(ang), math.sin(ang)
+        u = (xx - cx) * c + (yy - cy) * s
+        v = -(xx - cx) * s + (yy - cy) * c
+        rho = np.sqrt((u / a) ** 2 + (v / b) ** 2)
+        out[(rho >= 1.0) & (rho < 1.8)] = rng.uniform(8, 25)
+        out[rho < 1.0] = 254.0
+        markers.append((cx, cy, a, b, ang))
+    for _ in range(n_glints):
+        r = float(rng.uniform(3, 7))
+        cx, cy = float(rng.uniform(margin, w - margin)), float(rng.uniform(margin, h - margin))
+        if not free(cx, cy, 3 * r):
+            continue
+        placed.append((cx, cy, 3 * r))
+        d2 = (xx - cx) ** 2 + (yy - cy) ** 2
+        out[d2 < (3 * r) ** 2] = np.maximum(out[d2 < (3 * r) ** 2], 170.0)
+        out[d2 < r * r] = 240.0
+        glints.append((cx, cy, r))
+    for _ in range(n_dots):
+        cx, cy = float(rng.uniform(4, w - 4)), float(rng.uniform(4, h - 4))
+        if not free(cx, cy, 3):
+            continue
+        d2 = (xx - cx) ** 2 + (yy - cy) ** 2
+        out[d2 < 2.5 ** 2] = 200.0
+        dots.append((cx, cy))
+    out += rng.normal(0.0, 2.0, size=out.shape).astype(np.float32)
+    return np.clip(np.rint(out), 0, 255).astype(np.uint8), MarkerLayout(markers, glints, dots)

@@ -75,6 +75,24 @@ def build(ref: str | None = None) -> None:
     subprocess.run(cmd, check=True)
 
 
+class _BlobParams(C.Structure):
+    _fields_ = [("threshold", C.c_uint32), ("min_diameter", C.c_uint32), ("max_diameter", C.c_uint32),
+                ("max_aspect", C.c_float), ("min_fill", C.c_float), ("border", C.c_uint32), ("max_axis_ratio", C.c_float),
+                ("ring_scale", C.c_float), ("ring_contrast", C.c_float), ("ring_max_bright", C.c_float),
+                ("max_blobs", C.c_uint32)]
+
+
+def blob_params_c(bp=None) -> _BlobParams:
+    """orc_blob_params from an object with depth_metal::BlobParams' fields (defaults when None)."""
+    d = dict(threshold=150, min_diameter=3, max_diameter=60, max_aspect=4.0, min_fill=0.5, border=4, max_axis_ratio=3.0,
+             ring_scale=1.4, ring_contrast=0.5, ring_max_bright=0.3, max_blobs=1024)
+    if bp is not None:
+        d.update({k: getattr(bp, k) for k in d})
+    return _BlobParams(int(d["threshold"]), int(d["min_diameter"]), int(d["max_diameter"]), float(d["max_aspect"]),
+                       float(d["min_fill"]), int(d["border"]), float(d["max_axis_ratio"]), float(d["ring_scale"]),
+                       float(d["ring_contrast"]), float(d["ring_max_bright"]), int(d["max_blobs"]))
+
+
 class Port:
     """The C restatement (oracle/sgm_oracle.c)."""
 
@@ -97,6 +115,10 @@ class Port:
         L.orc_encode_u16.argtypes = [vp, C.c_long, i, vp]
         L.orc_points.argtypes = [vp, vp, i, i, d, d, d, d, d, f, f, f, f, f, vp, vp, vp]
         L.orc_pack_depth.argtypes = [vp, vp, i, i, vp]
+        L.orc_find_blobs.argtypes = [vp, i, i, i, vp, i]
+        L.orc_find_blobs.restype = i
+        L.orc_blob_candidates.argtypes = [vp, i, i, C.POINTER(_BlobParams), vp, i]
+        L.orc_blob_candidates.restype = i
 
     def census(self, img, rx=2, ry=2) -> np.ndarray:
         img = _u8(img)
@@ -174,6 +196,26 @@ class Port:
                             float(cx_offset), float(min_depth), float(max_depth), float(max_jump), float(edge_weight),
                             float(weight_reference_depth), _p(pts), _p(nrm), _p(wts))
         return pts, nrm, wts
+
+    def find_blobs(self, img, threshold=150) -> np.ndarray:
+        """markers::find_blobs restated (detect.cpp:14-45): (n, 12) int32 rows of x0, y0, x1, y1, pixels,
+        peak, first pixel, five moment sums, in the CPU detector's order."""
+        img = _u8(img)
+        h, w = img.shape
+        n = self.lib.orc_find_blobs(_p(img), w, h, int(threshold), None, 0)
+        out = np.zeros((max(n, 1), 12), np.int32)
+        self.lib.orc_find_blobs(_p(img), w, h, int(threshold), _p(out), n)
+        return out[:n]
+
+    def blob_candidates(self, img, params=None, cap=None):
+        """The GPU blob search's candidates restated: ((k, 6) uint32 boxes, number that passed)."""
+        img = _u8(img)
+        h, w = img.shape
+        bp = blob_params_c(params)
+        cap = int(bp.max_blobs if cap is None else cap)
+        out = np.zeros((max(cap, 1), 6), np.uint32)
+        n = self.lib.orc_blob_candidates(_p(img), w, h, C.byref(bp), _p(out), cap)
+        return out[:min(n, cap)], n
 
     def pack_depth(self, points_xyzw, weights) -> np.ndarray:
         """depth_metal::DepthPacker restated (depth_packer.cpp:10-21): w*h*3 bytes."""

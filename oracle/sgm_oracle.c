@@ -403,3 +403,146 @@ void orc_pack_depth(const float* points_xyzw, const float* weights, int w, int h
             out[2 * n + i] = (uint8_t)c;
         }
 }
+
+/* ---- marker blob search ---------------------------------------------------------------------------------- */
+
+/* Connected components above the threshold, libs/markers/src/detect.cpp:14-45: scan in raster order, flood
+ * fill each unlabelled foreground pixel with an explicit stack. */
+int orc_find_blobs(const uint8_t* img, int w, int h, int threshold, orc_blob* out, int cap) {
+    const size_t n = (size_t)w * (size_t)h;
+    int32_t* label = (int32_t*)malloc(n * sizeof(int32_t));
+    int* stack = (int*)malloc(n * sizeof(int));
+    if (!label || !stack) {
+        free(label);
+        free(stack);
+        return -1;
+    }
+    for (size_t i = 0; i < n; ++i) label[i] = -1;
+    int nb = 0;
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            const size_t i = (size_t)y * w + x;
+            if (img[i] <= threshold || label[i] >= 0) continue;
+            orc_blob b;
+            memset(&b, 0, sizeof(b));
+            b.x0 = b.x1 = x;
+            b.y0 = b.y1 = y;
+            b.root = (int32_t)i;
+            uint32_t m[5] = {0, 0, 0, 0, 0};
+            int top = 0;
+            stack[top++] = (int)i;
+            label[i] = nb;
+            while (top > 0) {
+                const int p = stack[--top];
+                const int px = p % w, py = p / w;
+                ++b.pixels;
+                if (img[p] > b.peak) b.peak = img[p];
+                b.x0 = imin(b.x0, px), b.x1 = imax(b.x1, px), b.y0 = imin(b.y0, py), b.y1 = imax(b.y1, py);
+                const int dx = px - x, dy = py - y;
+                m[0] += (uint32_t)dx, m[1] += (uint32_t)dy, m[2] += (uint32_t)(dx * dx), m[3] += (uint32_t)(dx * dy),
+                    m[4] += (uint32_t)(dy * dy);
+                const int nbr[4][2] = {{px - 1, py}, {px + 1, py}, {px, py - 1}, {px, py + 1}};
+                for (int k = 0; k < 4; ++k) {
+                    const int qx = nbr[k][0], qy = nbr[k][1];
+                    if (qx < 0 || qy < 0 || qx >= w || qy >= h) continue;
+                    const size_t j = (size_t)qy * w + qx;
+                    if (label[j] >= 0 || img[j] <= threshold) continue;
+                    label[j] = nb;
+                    stack[top++] = (int)j;
+                }
+            }
+            for (int k = 0; k < 5; ++k) b.mom[k] = (int32_t)m[k];
+            if (nb < cap) out[nb] = b;
+            ++nb;
+        }
+    free(label);
+    free(stack);
+    return nb;
+}
+
+static const float k_ring_cos[16] = {1.0f, 0.923879533f, 0.707106781f, 0.382683432f, 0.0f, -0.382683432f, -0.707106781f, -0.923879533f,
+                                     -1.0f, -0.923879533f, -0.707106781f, -0.382683432f, 0.0f, 0.382683432f, 0.707106781f, 0.923879533f};
+static const float k_ring_sin[16] = {0.0f, 0.382683432f, 0.707106781f, 0.923879533f, 1.0f, 0.923879533f, 0.707106781f, 0.382683432f,
+                                     0.0f, -0.382683432f, -0.707106781f, -0.923879533f, -1.0f, -0.923879533f, -0.707106781f, -0.382683432f};
+
+/* Grey level at the nearest pixel (round half away from zero), coordinates clamped before the conversion. */
+static float blob_sample(const uint8_t* img, int w, int h, float x, float y) {
+    x = fminf(fmaxf(x, -1.0f), (float)w);
+    y = fminf(fmaxf(y, -1.0f), (float)h);
+    const int sx = imin(imax((int)roundf(x), 0), w - 1), sy = imin(imax((int)roundf(y), 0), h - 1);
+    return (float)img[(size_t)sy * w + sx];
+}
+
+static float blob_ring(const uint8_t* img, int w, int h, int k, float su, float sv, float ct, float st, float cx, float cy) {
+    const float u = su * k_ring_cos[k], v = sv * k_ring_sin[k];
+    return blob_sample(img, w, h, (cx + ct * u) - st * v, (cy + st * u) + ct * v);
+}
+
+/* 1 when blob b passes the size, aspect, fill and border gates and the dark-ring pre-check. */
+static int blob_passes(const uint8_t* img, int w, int h, const orc_blob_params* p, const orc_blob* b) {
+    const float bw = (float)(b->x1 - b->x0 + 1), bh = (float)(b->y1 - b->y0 + 1);
+    const float dmin = (float)p->min_diameter, dmax = (float)p->max_diameter;
+    if (bw < dmin || bh < dmin || bw > dmax || bh > dmax) return 0;
+    if (fmaxf(bw, bh) > p->max_aspect * fminf(bw, bh)) return 0;
+    const float pi = 3.14159265358979f;
+    if ((float)b->pixels < (((p->min_fill * bw) * bh) * pi) / 4.0f) return 0;
+    const int m = imax(3, (int)fmaxf(bw, bh) / 2);
+    const int bd = (int)p->border;
+    if (b->x0 - m < bd || b->y0 - m < bd || b->x1 + m >= w - bd || b->y1 + m >= h - bd) return 0;
+    const float fn = (float)b->pixels;
+    const float mx = (float)b->mom[0] / fn, my = (float)b->mom[1] / fn;
+    const float cxx = (float)b->mom[2] / fn - mx * mx;
+    const float cxy = (float)b->mom[3] / fn - mx * my;
+    const float cyy = (float)b->mom[4] / fn - my * my;
+    const float dxy = cxx - cyy;
+    const float tr = 0.5f * (cxx + cyy);
+    const float det = sqrtf(fmaxf(0.0f, (0.25f * dxy) * dxy + cxy * cxy));
+    const float l1 = tr + det, l2 = fmaxf(tr - det, 0.0625f);
+    const float ea = 2.0f * sqrtf(fmaxf(l1, 0.0f)) + 0.5f, eb = 2.0f * sqrtf(l2) + 0.5f;
+    if (ea / eb > p->max_axis_ratio * 1.2f) return 0;
+    const float s2 = 2.0f * cxy;
+    const float r2 = sqrtf(dxy * dxy + s2 * s2);
+    float ct = 1.0f, st = 0.0f;
+    if (r2 > 0.0f) {
+        const float c2 = fminf(fmaxf(dxy / r2, -1.0f), 1.0f);
+        ct = sqrtf(0.5f * (1.0f + c2));
+        st = sqrtf(0.5f * (1.0f - c2));
+        if (s2 < 0.0f) st = -st;
+    }
+    const float cx = (float)(b->root % w) + mx, cy = (float)(b->root / w) + my;
+    float bg[16];
+    const float bu = 2.2f * ea, bv = 2.2f * eb;
+    for (int k = 0; k < 16; ++k) bg[k] = blob_ring(img, w, h, k, bu, bv, ct, st, cx, cy);
+    for (int a = 0; a < 4; ++a)
+        for (int q = a + 1; q < 16; ++q)
+            if (bg[q] < bg[a]) {
+                const float t = bg[a];
+                bg[a] = bg[q];
+                bg[q] = t;
+            }
+    const float level = bg[3] + p->ring_contrast * ((float)b->peak - bg[3]);
+    const float ru = p->ring_scale * ea, rv = p->ring_scale * eb;
+    int bright = 0;
+    for (int k = 0; k < 16; ++k) bright += blob_ring(img, w, h, k, ru, rv, ct, st, cx, cy) > level ? 1 : 0;
+    return (float)bright > p->ring_max_bright * 16.0f ? 0 : 1;
+}
+
+int orc_blob_candidates(const uint8_t* img, int w, int h, const orc_blob_params* p, uint32_t* boxes, int cap) {
+    const int nb = orc_find_blobs(img, w, h, (int)p->threshold, NULL, 0);
+    if (nb < 0) return -1;
+    orc_blob* blobs = (orc_blob*)malloc((size_t)(nb > 0 ? nb : 1) * sizeof(orc_blob));
+    if (!blobs) return -1;
+    orc_find_blobs(img, w, h, (int)p->threshold, blobs, nb);
+    int found = 0;
+    for (int i = 0; i < nb; ++i) {
+        if (!blob_passes(img, w, h, p, &blobs[i])) continue;
+        if (found < cap) {
+            uint32_t* o = boxes + 6 * (size_t)found;
+            o[0] = (uint32_t)blobs[i].x0, o[1] = (uint32_t)blobs[i].y0, o[2] = (uint32_t)blobs[i].x1, o[3] = (uint32_t)blobs[i].y1;
+            o[4] = (uint32_t)blobs[i].pixels, o[5] = (uint32_t)blobs[i].peak;
+        }
+        ++found;
+    }
+    free(blobs);
+    return found;
+}

@@ -61,6 +61,27 @@ void orc_points(const float* disp, const float* conf, int w, int h, double f, do
  * delta-coded along rows (q - q_left, mod 2^16), then u8 confidence round(w * 255); out = w*h*3 bytes. */
 void orc_pack_depth(const float* points_xyzw, const float* weights, int w, int h, uint8_t* out);
 
+/* Marker blob search. orc_find_blobs: connected pixels above `threshold` (4-neighbourhood), in the order
+ * and with the statistics of markers::find_blobs (libs/markers/src/detect.cpp:14-45), plus each blob's
+ * first pixel and its second moments relative to that pixel (32-bit two's complement sums). Returns the
+ * number of blobs; at most `cap` are written. orc_blob_candidates: the gates and dark-ring pre-check of
+ * the GPU search (stereo_kernels.metal.inc:846-900, restated with half-angle formulas and a table of the
+ * 16 ring directions) over those blobs, in the same order; returns the number that pass, at most `cap`
+ * written as (x0, y0, x1, y1, pixels, peak). */
+typedef struct orc_blob {
+    int32_t x0, y0, x1, y1, pixels, peak, root;
+    int32_t mom[5];
+} orc_blob;
+typedef struct orc_blob_params {
+    uint32_t threshold, min_diameter, max_diameter;
+    float max_aspect, min_fill;
+    uint32_t border;
+    float max_axis_ratio, ring_scale, ring_contrast, ring_max_bright;
+    uint32_t max_blobs;
+} orc_blob_params;
+int orc_find_blobs(const uint8_t* img, int w, int h, int threshold, orc_blob* out, int cap);
+int orc_blob_candidates(const uint8_t* img, int w, int h, const orc_blob_params* p, uint32_t* boxes, int cap);
+
 #ifdef __cplusplus
 }
 #endif

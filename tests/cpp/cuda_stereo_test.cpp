@@ -79,7 +79,12 @@ int main(int argc, char** argv) {
     }
     pyr.pyramid_levels = 5;
     if (auto c = depth_cuda::CudaStereo::create(pyr, w, h); c || c.error().code != depth_cuda::Errc::invalid_argument) bad = 1;
-    // compute_raw before set_rectification: invalid_argument (metal_stereo.cpp:343)
+    // marker blob search: find_blobs before set_blob_params is invalid_argument; afterwards it runs
+    if (auto b = (*s)->find_blobs(l); b || b.error().code != depth_cuda::Errc::invalid_argument) bad = 1;
+    if (!(*s)->set_blob_params({})) bad = 1;
+    std::uint32_t found = 0;
+    if (auto b = (*s)->find_blobs(l, &found); !b || b->size() != std::min<std::uint32_t>(found, 1024)) bad = 1;
+        // compute_raw before set_rectification: invalid_argument (metal_stereo.cpp:343)
     if (auto res = (*s)->compute_raw(l, r); res || res.error().code != depth_cuda::Errc::invalid_argument) bad = 1;
     std::printf(bad ? "FAIL\n" : "OK\n");
     return bad;
