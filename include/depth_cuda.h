@@ -295,6 +295,13 @@ DS_API int ds_disparity_to_points(const float* disparity, const float* confidenc
 DS_API int ds_pack_depth(const float* points_xyzw, const float* weights, int width, int height, uint8_t* packed,
                          void* stream);
 
+/* Raw IR images of a session recording (the RAWI record, libs/session/src/session.cpp:248-272, read back at
+ * :815-836): after zstd decompression each row holds its bytes delta-coded from the left neighbour (mod 256).
+ * Undoes that on the device, `coded` -> `image` (width x height, rows `*_stride` bytes apart), enqueued on
+ * `stream`. In place when coded == image (equal strides); otherwise the buffers must not overlap. */
+DS_API int ds_undelta_rows(const uint8_t* coded, ptrdiff_t coded_stride, uint8_t* image, ptrdiff_t image_stride, int width, int height,
+                           void* stream);
+
 /* ---- Marker blob search on the raw images -------------------------------------------------------------
  * depth_metal::BlobParams / BlobBox (metal_stereo.hpp:21-39) and MetalStereo::set_blob_params /
  * FrameRequest::marker_blobs (metal_stereo.hpp:41-58, 94-95): connected pixels above `threshold`

@@ -139,6 +139,7 @@ SIGNATURES = {
     "ds_default_point_params": (None, [C.POINTER(PointParamsC)]),
     "ds_disparity_to_points": (_i, [_vp, _vp, _i, _i, C.POINTER(GeometryC), C.POINTER(PointParamsC), _vp, _vp, _vp, _vp]),
     "ds_pack_depth": (_i, [_vp, _vp, _i, _i, _vp, _vp]),
+    "ds_undelta_rows": (_i, [_vp, C.c_ssize_t, _vp, C.c_ssize_t, _i, _i, _vp]),
     "ds_default_blob_params": (None, [C.POINTER(BlobParamsC)]),
     "ds_set_blob_params": (_i, [_vp, C.POINTER(BlobParamsC)]),
     "ds_compute_raw_blobs": (_i, [_vp, _vp, _vp, C.c_ssize_t, C.POINTER(OutputsC), C.POINTER(BlobBoxesC)]),

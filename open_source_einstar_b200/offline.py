@@ -76,11 +76,13 @@ class OfflineRedepth:
     def device_bytes(self) -> int:
         return sum(b.device_bytes for b in self.batches)
 
-    def run(self, left_frames, right_frames, out_u16: np.ndarray, out_depth: np.ndarray | None = None) -> OfflineStats:
+    def run(self, left_frames, right_frames, out_u16: np.ndarray, out_depth: np.ndarray | None = None,
+            delta_coded: bool = False) -> OfflineStats:
         """Re-depths frames[i] for all i. left_frames/right_frames: sequences of host u8 raw images (pinned
         for overlap). out_u16 (N x H x W, uint16) and out_depth (N x H x W, float32) receive the results;
         pinned host arrays let the copies overlap the next batch. A last partial batch is padded with its
-        final frame."""
+        final frame. With `delta_coded`, the images are a session recording's row-delta-coded bytes
+        (recording.py) and are decoded on the GPU after their upload, on the copy stream."""
         torch = self.torch
         N = len(left_frames)
         nb = (N + self.n - 1) // self.n
@@ -97,6 +99,10 @@ class OfflineRedepth:
                     i = min(k * self.n + j, N - 1)
                     self.inputs[s][j][0].copy_(torch.from_numpy(np.asarray(left_frames[i])), non_blocking=True)
                     self.inputs[s][j][1].copy_(torch.from_numpy(np.asarray(right_frames[i])), non_blocking=True)
+                    if delta_coded:
+                        from .recording import undelta_rows
+                        for img in self.inputs[s][j]:
+                            undelta_rows(img, img, self.copy)
                 self.h2d_done[s].record(self.copy)
 
         def download(k):
