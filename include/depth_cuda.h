@@ -347,6 +347,29 @@ DS_API int ds_set_blob_params(ds_handle* handle, const ds_blob_params* params);
  * stereo (MetalStereo::compute_frame with FrameRequest::marker_blobs). */
 DS_API int ds_compute_raw_blobs(ds_handle* handle, const uint8_t* raw_left, const uint8_t* raw_right, ptrdiff_t stride,
                                 const ds_outputs* out, ds_blob_boxes* blobs);
+/* MetalStereo::compute_frame (metal_stereo.hpp:88-91 with FrameRequest / FrameOutputs, :41-58), the call the
+ * scanner frontend makes per frame (libs/pipeline/src/stereo_frontend.cpp:302-328): raw pair in; the
+ * frame's points, normals and weights (ds_disparity_to_points with the handle's point parameters and the
+ * default ds_point_params otherwise) written to the caller's device buffers and left there; optional host
+ * copies (`host`: disparity, confidence, u16, depth, rectified pair); with `marker_blobs`, the blob
+ * candidates of both raw images in `blobs`, handed to `on_blobs` (when set) on the calling thread as soon as
+ * the blob search has finished, while the stereo may still run on the GPU. */
+typedef void (*ds_blob_callback)(const ds_blob_boxes* blobs, void* user);
+typedef struct ds_frame_request {
+    int marker_blobs;          /* needs ds_set_blob_params */
+    ds_blob_callback on_blobs; /* may be NULL */
+    void* user;
+} ds_frame_request;
+typedef struct ds_frame_outputs {
+    float* points_xyzw;        /* device, W*H float4 (16-byte aligned); with normals and weights, or all NULL */
+    float* normals_xyzw;       /* device, W*H float4 */
+    float* weights;            /* device, W*H */
+    ds_outputs host;           /* host copies; entries may be NULL */
+    ds_blob_boxes* blobs;      /* host; needed with marker_blobs */
+} ds_frame_outputs;
+DS_API int ds_compute_frame(ds_handle* handle, const uint8_t* raw_left, const uint8_t* raw_right, ptrdiff_t stride,
+                            const ds_frame_request* request, ds_frame_outputs* out);
+
 /* The blob search alone on one host image of any size (width x height, rows `stride` bytes apart):
  * up to `capacity` boxes, `found` = candidates that passed. Needs ds_set_blob_params. */
 DS_API int ds_find_blobs(ds_handle* handle, const uint8_t* image, int width, int height, ptrdiff_t stride, ds_blob_box* out,

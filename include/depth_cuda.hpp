@@ -11,6 +11,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <expected>
+#include <functional>
 #include <memory>
 #include <string>
 #include <utility>
@@ -142,6 +143,19 @@ struct StereoResult {
     std::array<std::uint32_t, 2> blobs_found{};
 };
 
+// depth_metal::FrameRequest (metal_stereo.hpp:41-50), the parts a CUDA frame has.
+struct FrameRequest {
+    bool marker_blobs = false;
+    std::function<void(const std::array<std::vector<BlobBox>, 2>&)> on_blobs;
+};
+
+// The device buffers a frame's points, normals (float4 per pixel) and weights go to (gpu::MetalFrameData).
+struct DeviceFrame {
+    float* points_xyzw = nullptr;
+    float* normals_xyzw = nullptr;
+    float* weights = nullptr;
+};
+
 class CudaStereo {
 public:
     static Result<std::unique_ptr<CudaStereo>> create(const StereoParams& p, int width, int height) {
@@ -191,6 +205,53 @@ public:
     // Raw pair -> stereo, with the marker blob search on both raw images (FrameRequest::marker_blobs).
     Result<StereoResult> compute_raw_blobs(ImageViewU8 raw_left, ImageViewU8 raw_right) {
         return run(raw_left, raw_right, true, nullptr, nullptr, true);
+    }
+
+    // MetalStereo::compute_frame, the frontend's per-frame call: raw pair in; points, normals (float4 per pixel)
+    // and weights written to the caller's device buffers (all three, or none); the host result as compute_raw;
+    // with marker_blobs, the candidates in res.blobs, and on_blobs called with them (on this thread) as soon
+    // as the blob search has finished, while the stereo may still run.
+    Result<StereoResult> compute_frame(ImageViewU8 raw_left, ImageViewU8 raw_right, const FrameRequest& req, DeviceFrame frame = {}) {
+        if (!raw_left.data || !raw_right.data || raw_left.stride != raw_right.stride)
+            return std::unexpected(Error{Errc::invalid_argument, "null images or different strides"});
+        const std::size_t n = static_cast<std::size_t>(w_) * h_px_;
+        StereoResult res;
+        res.width = w_;
+        res.height = h_px_;
+        res.disparity.resize(n);
+        res.confidence.resize(n);
+        res.disparity_u16.resize(n);
+        if (have_points_) res.depth.resize(n);
+        ds_frame_outputs o{};
+        o.points_xyzw = frame.points_xyzw;
+        o.normals_xyzw = frame.normals_xyzw;
+        o.weights = frame.weights;
+        o.host = ds_outputs{res.disparity.data(), res.confidence.data(), res.disparity_u16.data(), have_points_ ? res.depth.data() : nullptr,
+                            nullptr, nullptr};
+        ds_blob_boxes bb{};
+        struct Ctx {
+            const FrameRequest* req;
+            StereoResult* res;
+        } ctx{&req, &res};
+        ds_frame_request r{};
+        if (req.marker_blobs) {
+            res.blobs[0].resize(max_blobs_);
+            res.blobs[1].resize(max_blobs_);
+            bb = ds_blob_boxes{res.blobs[0].data(), res.blobs[1].data(), max_blobs_, {0, 0}, {0, 0}};
+            o.blobs = &bb;
+            r.marker_blobs = 1;
+            r.user = &ctx;
+            r.on_blobs = [](const ds_blob_boxes* b, void* user) {
+                auto* c = static_cast<Ctx*>(user);
+                c->res->blobs[0].resize(b->kept[0]);
+                c->res->blobs[1].resize(b->kept[1]);
+                c->res->blobs_found = {b->found[0], b->found[1]};
+                if (c->req->on_blobs) c->req->on_blobs(c->res->blobs);
+            };
+        }
+        if (const int rc = ds_compute_frame(h_, raw_left.data, raw_right.data, raw_left.stride, &r, &o); rc != DS_OK)
+            return std::unexpected(Error{static_cast<Errc>(rc), ds_last_error(h_)});
+        return res;
     }
 
     // The blob search alone on one image: candidates ordered by first pixel.

@@ -80,6 +80,18 @@ class BlobBoxesC(C.Structure):
                 ("kept", C.c_uint32 * 2)]
 
 
+BLOB_CALLBACK = C.CFUNCTYPE(None, C.POINTER(BlobBoxesC), C.c_void_p)
+
+
+class FrameRequestC(C.Structure):
+    _fields_ = [("marker_blobs", C.c_int), ("on_blobs", BLOB_CALLBACK), ("user", C.c_void_p)]
+
+
+class FrameOutputsC(C.Structure):
+    _fields_ = [("points_xyzw", C.c_void_p), ("normals_xyzw", C.c_void_p), ("weights", C.c_void_p), ("host", OutputsC),
+                ("blobs", C.POINTER(BlobBoxesC))]
+
+
 class ServerOptionsC(C.Structure):
     _fields_ = [("volume_budget_bytes", C.c_size_t), ("max_slots", C.c_int), ("max_pending", C.c_int)]
 
@@ -143,6 +155,7 @@ SIGNATURES = {
     "ds_default_blob_params": (None, [C.POINTER(BlobParamsC)]),
     "ds_set_blob_params": (_i, [_vp, C.POINTER(BlobParamsC)]),
     "ds_compute_raw_blobs": (_i, [_vp, _vp, _vp, C.c_ssize_t, C.POINTER(OutputsC), C.POINTER(BlobBoxesC)]),
+    "ds_compute_frame": (_i, [_vp, _vp, _vp, C.c_ssize_t, C.POINTER(FrameRequestC), C.POINTER(FrameOutputsC)]),
     "ds_find_blobs": (_i, [_vp, _vp, _i, _i, C.c_ssize_t, _vp, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "ds_server_create": (_i, [C.POINTER(ServerOptionsC), C.POINTER(_vp)]),
     "ds_server_destroy": (None, [_vp]),

@@ -765,8 +765,19 @@ int blob_finish(ds_handle* h, const BlobHost& hb, ds_blob_box* out, uint32_t cap
     return DS_OK;
 }
 
+// What a ds_compute_frame call adds to a host frame: blob search outputs and their callback, device points.
+struct FrameExtras {
+    ds_blob_boxes* blobs = nullptr;
+    ds_blob_callback on_blobs = nullptr;
+    void* user = nullptr;
+    float* points = nullptr;   // device, W*H float4 each (points, normals), W*H weights
+    float* normals = nullptr;
+    float* weights = nullptr;
+};
+
 int run_host(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t stride, const ds_outputs* out, bool raw,
-             ds_blob_boxes* blobs = nullptr) {
+             const FrameExtras* fx = nullptr) {
+    ds_blob_boxes* blobs = fx ? fx->blobs : nullptr;
     const double t0 = now_ms();
     const int iw = raw ? h->raw_w : h->w, ih = raw ? h->raw_h : h->h;
     if (!left || !right) return h->fail(DS_INVALID_ARGUMENT, "null image");
@@ -788,6 +799,17 @@ int run_host(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t 
         }
     }
     enqueue_frame(h, dst[0], dst[1], raw, internal_outputs(h), h->stream);
+    if (fx && fx->points) {  // the frame's points, normals and weights stay on the device
+        ds_point_params pp{};
+        ds_default_point_params(&pp);
+        pp.min_depth_mm = h->min_depth;
+        pp.max_depth_mm = h->max_depth;
+        pp.max_depth_jump_mm = h->max_jump;
+        if (const int rc = ds_disparity_to_points(h->d_out_disp, h->d_out_conf, h->w, h->h, &h->geom, &pp, fx->points, fx->normals,
+                                                  fx->weights, h->stream);
+            rc != DS_OK)
+            return h->fail(rc, ds_last_global_error());
+    }
     DS_CUDA(cudaEventRecord(h->ev1, h->stream));
     const size_t n = static_cast<size_t>(h->w) * h->h;
     if (out) {
@@ -798,13 +820,18 @@ int run_host(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t 
         if (out->rect_left) DS_CUDA(cudaMemcpyAsync(out->rect_left, h->d_rect[0], n, cudaMemcpyDeviceToHost, h->stream));
         if (out->rect_right) DS_CUDA(cudaMemcpyAsync(out->rect_right, h->d_rect[1], n, cudaMemcpyDeviceToHost, h->stream));
     }
-    DS_CUDA(cudaStreamSynchronize(h->stream));
-    if (blobs) {
+    if (blobs) {  // the candidates are handed over while the stereo may still run
         DS_CUDA(cudaStreamSynchronize(h->blob_stream));
         ds_blob_box* bo[2] = {blobs->left, blobs->right};
-        for (int s = 0; s < 2; ++s)
-            if (const int rc = blob_finish(h, bh[s], bo[s], blobs->capacity, &blobs->found[s], &blobs->kept[s]); rc != DS_OK) return rc;
+        int rc = DS_OK;
+        for (int s = 0; s < 2 && rc == DS_OK; ++s) rc = blob_finish(h, bh[s], bo[s], blobs->capacity, &blobs->found[s], &blobs->kept[s]);
+        if (rc != DS_OK) {
+            DS_CUDA(cudaStreamSynchronize(h->stream));
+            return rc;
+        }
+        if (fx->on_blobs) fx->on_blobs(blobs, fx->user);
     }
+    DS_CUDA(cudaStreamSynchronize(h->stream));
     if (h->refine && h->p.speckle_max_region_size > 1) {
         int err = 0;
         DS_CUDA(cudaMemcpy(&err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1293,7 +1320,34 @@ DS_API int ds_compute_raw_blobs(ds_handle* h, const uint8_t* left, const uint8_t
     if (!h->have_rect) return h->fail(DS_INVALID_ARGUMENT, "set_rectification() not called");
     if (!blobs || !blobs->left || !blobs->right) return h->fail(DS_INVALID_ARGUMENT, "null blob outputs");
     if (!h->have_blobs) return h->fail(DS_INVALID_ARGUMENT, "set_blob_params() not called");
-    return guarded(h, [&] { return run_host(h, left, right, stride, out, true, blobs); });
+    FrameExtras fx;
+    fx.blobs = blobs;
+    return guarded(h, [&] { return run_host(h, left, right, stride, out, true, &fx); });
+}
+
+DS_API int ds_compute_frame(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t stride, const ds_frame_request* req,
+                            ds_frame_outputs* out) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    if (!out) return h->fail(DS_INVALID_ARGUMENT, "null frame outputs");
+    if (!h->have_rect) return h->fail(DS_INVALID_ARGUMENT, "set_rectification() not called");
+    FrameExtras fx;
+    const bool any_points = out->points_xyzw || out->normals_xyzw || out->weights;
+    if (any_points) {
+        if (!out->points_xyzw || !out->normals_xyzw || !out->weights)
+            return h->fail(DS_INVALID_ARGUMENT, "points, normals and weights are produced together");
+        if (!h->have_points) return h->fail(DS_INVALID_ARGUMENT, "set_point_params() not called");
+        fx.points = out->points_xyzw;
+        fx.normals = out->normals_xyzw;
+        fx.weights = out->weights;
+    }
+    if (req && req->marker_blobs) {
+        if (!h->have_blobs) return h->fail(DS_INVALID_ARGUMENT, "set_blob_params() not called");
+        if (!out->blobs || !out->blobs->left || !out->blobs->right) return h->fail(DS_INVALID_ARGUMENT, "null blob outputs");
+        fx.blobs = out->blobs;
+        fx.on_blobs = req->on_blobs;
+        fx.user = req->user;
+    }
+    return guarded(h, [&] { return run_host(h, left, right, stride, &out->host, true, &fx); });
 }
 
 DS_API int ds_find_blobs(ds_handle* h, const uint8_t* image, int width, int height, ptrdiff_t stride, ds_blob_box* out,

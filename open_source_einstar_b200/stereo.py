@@ -342,6 +342,45 @@ class CudaStereo:
         res.blobs_found = (int(bb.found[0]), int(bb.found[1]))
         return res
 
+    def compute_frame(self, raw_left: np.ndarray, raw_right: np.ndarray, points=None, normals=None, weights=None,
+                      blobs: bool = False, on_blobs=None, rectified: bool = False) -> StereoResult:
+        """MetalStereo::compute_frame (metal_stereo.hpp:88-91), the scanner frontend's per-frame call: raw pair
+        in; points / normals (H x W x 4 float32) and weights (H x W float32), device tensors of the caller,
+        receive the frame and stay on the device; the host result holds disparity, confidence, u16 (and
+        depth, the rectified pair) as compute_raw. With `blobs`, res.blobs has the marker candidates, and
+        `on_blobs(left, right)` (if given) is called with them while the stereo may still run."""
+        if self.raw_size is None:
+            raise StereoError(Errc.invalid_argument, "set_rectification() not called")
+        rw, rh = self.raw_size
+        raw_left = _check_u8(raw_left, rw, rh, "raw left")
+        raw_right = _check_u8(raw_right, rw, rh, "raw right")
+        if raw_left.strides[0] != raw_right.strides[0]:
+            raw_left, raw_right = np.ascontiguousarray(raw_left), np.ascontiguousarray(raw_right)
+        res, o = self._outputs(rectified)
+        fo = N.FrameOutputsC(_ptr(points), _ptr(normals), _ptr(weights), o, None)
+        req = N.FrameRequestC(0, N.BLOB_CALLBACK(), None)
+        keep = []
+        if blobs:
+            if self.blob_params is None:
+                raise StereoError(Errc.invalid_argument, "set_blob_params() not called")
+            cap = self.blob_params.max_blobs
+            bl, br = np.zeros((cap, 6), np.uint32), np.zeros((cap, 6), np.uint32)
+            bb = N.BlobBoxesC(bl.ctypes.data, br.ctypes.data, cap)
+            fo.blobs = C.pointer(bb)
+            req.marker_blobs = 1
+            if on_blobs is not None:
+                def cb(p, _user):
+                    b = p.contents
+                    on_blobs(bl[:b.kept[0]].copy(), br[:b.kept[1]].copy())
+                req.on_blobs = N.BLOB_CALLBACK(cb)
+                keep.append(req.on_blobs)
+        self._check(N.lib().ds_compute_frame(self._h, raw_left.ctypes.data, raw_right.ctypes.data, raw_left.strides[0],
+                                             C.byref(req), C.byref(fo)))
+        if blobs:
+            res.blobs = (bl[:bb.kept[0]].copy(), br[:bb.kept[1]].copy())
+            res.blobs_found = (int(bb.found[0]), int(bb.found[1]))
+        return res
+
     def set_blob_params(self, params: "BlobParams | None" = None) -> None:
         """MetalStereo::set_blob_params (metal_stereo.cpp:279-291)."""
         params = params or BlobParams()
