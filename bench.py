@@ -535,6 +535,22 @@ def run_frontend(args, world, rank, local):
     for i in range(n_frames):
         res[0] = s.compute_raw(*host[i % B])
     e2e_s = time.perf_counter() - t0
+    # the frontend's own per-frame call (ds_compute_frame): points, normals and weights left on the device,
+    # marker blobs of both raw images (stickers composited into the scenes) handed over during the stereo
+    from open_source_einstar_b200 import BlobParams, RectifiedGeometry, synth
+    s.set_point_params(RectifiedGeometry(pairs[0].f / 2, (w - 1) / 2.0, (h - 1) / 2.0, pairs[0].baseline, 0.0), 150.0, 700.0, 4.0)
+    s.set_blob_params(BlobParams())
+    marked = [(synth.add_markers((p.left * 0.6).astype(np.uint8), n_markers=20, seed=2 * k)[0],
+               synth.add_markers((p.right * 0.6).astype(np.uint8), n_markers=20, seed=2 * k + 1)[0]) for k, p in enumerate(pairs[:2])]
+    pts = torch.empty((h, w, 4), dtype=torch.float32, device=dev)
+    nrm = torch.empty((h, w, 4), dtype=torch.float32, device=dev)
+    wts = torch.empty((h, w), dtype=torch.float32, device=dev)
+    fr = s.compute_frame(*marked[0], pts, nrm, wts, blobs=True)
+    t0 = time.perf_counter()
+    for i in range(n_frames):
+        fr = s.compute_frame(*marked[i % 2], pts, nrm, wts, blobs=True)
+    frame_s = time.perf_counter() - t0
+    blob_counts = [len(fr.blobs[0]), len(fr.blobs[1])]
     clk.__exit__(None, None, None)
     s.close()
     frame_tot = stages.sum(axis=1)
@@ -573,6 +589,12 @@ def run_frontend(args, world, rank, local):
                         "d2h_bytes_per_step": B * w * h * 8,
                         "api": "CudaStereo.compute_raw (ds_compute_raw): host raw pair in, host disparity + confidence out, "
                                "wall clock"},
+                "e2e_frame": {"value": n_frames / frame_s, "unit": "frames/s", "h2d_bytes_per_step": B * 2 * W * H,
+                              "d2h_bytes_per_step": B * w * h * 10,
+                              "api": "CudaStereo.compute_frame (ds_compute_frame): host raw pair in; points, normals, weights "
+                                     "left on the device; disparity, confidence, u16 and the marker candidates of both raw "
+                                     "images (20 stickers each) back on the host; wall clock",
+                              "marker_candidates": blob_counts},
                 "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     return 0
