@@ -123,6 +123,20 @@ def dist_setup():
     return world, rank, local
 
 
+def replica_seed0(rank: int) -> int:
+    """First scene seed of rank `rank`'s frames: replicas render disjoint scenes (no data-path collective)."""
+    return 100 * rank
+
+
+def max_over_ranks(v: float, world: int, device) -> float:
+    """The slowest rank's time (or any per-rank value): one all-reduce MAX in float64 over the job."""
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def make_frames(n, seed0, device):
     from open_source_einstar_b200 import synth
     pairs = [synth.raw_objects_pair(seed=seed0 + i, device=device) for i in range(n)]
@@ -489,7 +503,7 @@ def run_frontend(args, world, rank, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     B = args.frames
-    pairs = make_frames(B, 100 * rank, dev)
+    pairs = make_frames(B, replica_seed0(rank), dev)
     (lx, ly), (rx, ry) = pairs[0].maps
     sp = frontend_params(pairs[0].f, pairs[0].baseline)
     w, h = W // 2, H // 2
@@ -644,7 +658,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
     B = args.frames
-    pairs = make_frames(B, 100 * rank, dev)
+    pairs = make_frames(B, replica_seed0(rank), dev)
     (lx, ly), (rx, ry) = pairs[0].maps
     sp = StereoParams(sgm=SgmParams(min_disparity=pairs[0].min_disparity, num_disparities=D))
     geom = RectifiedGeometry(pairs[0].f, 0, 0, pairs[0].baseline, 0.0)
@@ -663,11 +677,8 @@ def main():
             torch.distributed.barrier()
         torch.cuda.synchronize(dev)
 
-    def max_over_ranks(v: float) -> float:
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+    def job_max(v: float) -> float:
+        return max_over_ranks(v, world, dev)
 
     clk = ClockSampler(local).__enter__()
 
@@ -694,7 +705,7 @@ def main():
         frame_step()
     e1.record(stream)
     barrier()
-    pf_ms = max_over_ranks(e0.elapsed_time(e1))
+    pf_ms = job_max(e0.elapsed_time(e1))
     stages = s.profile_collect(max_frames=B * args.steps + 8)
     s.profile(False)
     frame_tot = stages.sum(axis=1) if len(stages) else np.zeros(1)
@@ -723,7 +734,7 @@ def main():
     e1.record(stream)
     barrier()
     launches = batch.launches_per_run * args.steps  # graph replays launch the captured kernels
-    ms = max_over_ranks(e0.elapsed_time(e1))
+    ms = job_max(e0.elapsed_time(e1))
     bstage = batch.stage_ms()
     frames_total = B * args.steps * world
     value = frames_total * PX_D / (ms * 1e-3) / 1e9
@@ -748,7 +759,7 @@ def main():
     off.run(e2e_l[:2 * B], e2e_r[:2 * B], e2e_u16[:2 * B], e2e_depth[:2 * B])  # warm-up (graph capture)
     barrier()
     est = off.run(e2e_l, e2e_r, e2e_u16, e2e_depth)
-    e2e_s = max_over_ranks(est.device_ms) * 1e-3
+    e2e_s = job_max(est.device_ms) * 1e-3
     e2e_value = n_e2e * world * PX_D / e2e_s / 1e9
     for j in range(B):  # the last step's results, copied out, equal the per-frame path's
         if not np.array_equal(e2e_u16[n_e2e - B + j], outs[j]["disparity_u16"].cpu().numpy().view(np.uint16)):
