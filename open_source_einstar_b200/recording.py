@@ -223,23 +223,35 @@ class SessionRawWriter:
 
 
 def replay(reader: SessionRawReader, redepth, out_u16: np.ndarray, out_depth: np.ndarray | None = None, left_sensor: int = 0,
-           threads: int = 8):
-    """Re-depths every RAWI frame of `reader` through `redepth` (an OfflineRedepth): zstd on `threads` host
-    threads, the row-delta decode on the GPU as part of each batch's upload. Frame i's images are the
-    sensors `left_sensor` and the other one. Returns the OfflineStats."""
-    n = len(reader)
+           threads: int = 8, chunk_batches: int = 4):
+    """Re-depths every RAWI frame of `reader` through `redepth` (an OfflineRedepth) into out_u16[i] /
+    out_depth[i]: zstd on `threads` host threads, the row-delta decode on the GPU as part of each batch's
+    upload. Frame i's images are the sensor `left_sensor` and the other one. Frames go through in chunks of
+    `chunk_batches` batches, so host memory stays bounded for long recordings. Returns the OfflineStats
+    summed over the chunks."""
+    from .offline import OfflineStats
     from .serving import pinned_empty
+    n = len(reader)
     h, w = redepth.raw_h, redepth.raw_w
-    lefts, rights = pinned_empty((n, h, w), np.uint8), pinned_empty((n, h, w), np.uint8)
+    chunk = max(1, chunk_batches) * redepth.n
+    lefts, rights = pinned_empty((min(chunk, n), h, w), np.uint8), pinned_empty((min(chunk, n), h, w), np.uint8)
 
-    def load(i):
+    def load(i, slot):
         f = reader.read_coded(i)
         imgs = dict(f.images)
         if left_sensor not in imgs or len(imgs) != 2:
             raise ValueError(f"raw frame {i}: expected two images including sensor {left_sensor}")
         right_sensor = next(s for s in imgs if s != left_sensor)
-        lefts[i], rights[i] = imgs[left_sensor], imgs[right_sensor]
+        if imgs[left_sensor].shape != (h, w) or imgs[right_sensor].shape != (h, w):
+            raise ValueError(f"raw frame {i}: images are not {w}x{h}")
+        lefts[slot], rights[slot] = imgs[left_sensor], imgs[right_sensor]
 
+    total = OfflineStats(0, 0, 0.0, 0)
     with ThreadPoolExecutor(max_workers=threads) as pool:
-        list(pool.map(load, range(n)))
-    return redepth.run(lefts, rights, out_u16, out_depth, delta_coded=True)
+        for start in range(0, n, chunk):
+            m = min(chunk, n - start)
+            list(pool.map(lambda k: load(start + k, k), range(m)))
+            st = redepth.run(lefts[:m], rights[:m], out_u16[start:start + m],
+                             None if out_depth is None else out_depth[start:start + m], delta_coded=True)
+            total = OfflineStats(total.frames + st.frames, total.batches + st.batches, total.device_ms + st.device_ms, st.device_bytes)
+    return total

@@ -81,7 +81,7 @@ def test_replay_recording_matches_per_frame_path(cuda, tmp_path):
     u16 = np.zeros((5, 512, 640), np.uint16)
     depth = np.zeros((5, 512, 640), np.float32)
     with OfflineRedepth(640, 512, sp, pairs[0].maps, (640, 512), geom, batch_size=2) as off:
-        st = R.replay(reader, off, u16, depth, left_sensor=0, threads=2)
+        st = R.replay(reader, off, u16, depth, left_sensor=0, threads=2, chunk_batches=1)  # chunks of 2 frames
     assert st.frames == 5
     with CudaStereo.create(sp, 640, 512) as s:
         s.set_rectification(RemapTable(lx, ly), RemapTable(rx, ry), 640, 512)
