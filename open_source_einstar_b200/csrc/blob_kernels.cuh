@@ -59,15 +59,14 @@ static __global__ void k_blob_init(BlobArgs a) {
     m[0] = m[1] = m[2] = m[3] = m[4] = 0;
 }
 
-// 4-neighbour links between foreground pixels.
-static __global__ void k_blob_union(BlobArgs a) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= a.w || y >= a.h) return;
-    const int i = y * a.w + x;
-    if (a.img[i] <= a.threshold) return;
-    if (x + 1 < a.w && a.img[i + 1] > a.threshold) uf_union(a.parent, i, i + 1, a.err);
-    if (y + 1 < a.h && a.img[i + a.w] > a.threshold) uf_union(a.parent, i, i + a.w, a.err);
-}
+// Blobs: pixels above the threshold, 4-neighbours linked.
+struct BlobConn {
+    const uint8_t* img;
+    int w;
+    uint32_t threshold;
+    __device__ __forceinline__ bool active(int x, int y) const { return img[static_cast<size_t>(y) * w + x] > threshold; }
+    __device__ __forceinline__ bool link(int, int, int x2, int y2) const { return active(x2, y2); }
+};
 
 // Per-root statistics. Lanes of a warp with the same root reduce first (one set of atomics per root and
 // warp): a bright surface under the ring light is one large component.

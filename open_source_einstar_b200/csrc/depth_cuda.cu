@@ -640,11 +640,12 @@ void enqueue_refine(ds_handle* h, const uint8_t* left, const uint8_t* right, boo
     if (p.speckle_max_region_size > 1) {
         const int nn = static_cast<int>(n), bl = (nn + 255) / 256;
         DS_CUDA(cudaMemsetAsync(h->d_err, 0, sizeof(int), st));
-        dsk::k_speckle_init<<<bl, 256, 0, st>>>(dcur, nn, h->d_parent, h->d_size);
-        dsk::k_speckle_union<<<grid2(w, ht), b2, 0, st>>>(dcur, w, ht, p.speckle_max_diff, h->d_parent, h->d_err);
+        DS_CUDA(cudaMemsetAsync(h->d_size, 0, n * sizeof(int), st));
+        const dsk::SpeckleConn conn{dcur, w, p.speckle_max_diff};
+        g_launches += dsk::launch_ccl(conn, w, ht, h->d_parent, h->d_err, st);
         dsk::k_speckle_count<<<bl, 256, 0, st>>>(dcur, nn, h->d_parent, h->d_size, h->d_err);
         dsk::k_speckle_apply<<<bl, 256, 0, st>>>(dcur, nn, h->d_parent, h->d_size, p.speckle_max_region_size, h->d_err);
-        g_launches += 4;
+        g_launches += 2;
     }
     enqueue_post(h, dcur, L > 0 ? h->d_rconf : nullptr, 0, out, st);
     marks.mark(6);
@@ -733,10 +734,11 @@ void enqueue_blob_search(ds_handle* h, int side, const uint8_t* img, int w, int 
     DS_CUDA(cudaMemsetAsync(b.n_out, 0, 2 * sizeof(uint32_t), st));
     const int n = w * ht, bl = (n + 255) / 256;
     dsk::k_blob_init<<<bl, 256, 0, st>>>(a);
-    dsk::k_blob_union<<<dim3((w + 31) / 32, (ht + 7) / 8), dim3(32, 8), 0, st>>>(a);
+    const dsk::BlobConn conn{img, w, bp.threshold};
+    g_launches += dsk::launch_ccl(conn, w, ht, a.parent, a.err, st);
     dsk::k_blob_stats<<<bl, 256, 0, st>>>(a);
     dsk::k_blob_select<<<bl, 256, 0, st>>>(a);
-    g_launches += 4;
+    g_launches += 3;
     DS_CUDA(cudaGetLastError());
 }
 

@@ -482,29 +482,17 @@ static __global__ void k_filter_spikes(const float* __restrict__ in, int w, int 
 // ---- speckle removal (stereo.cpp:465-494) as connected components by union-find -------------------------
 // Regions are connected under |d_a - d_b| <= max_diff between 4-neighbours, which is symmetric, so the
 // components (and therefore the removed pixels) do not depend on the order the reference visits them.
-static __global__ void k_speckle_init(const float* __restrict__ disp, int n, int* __restrict__ parent, int* __restrict__ size) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    parent[i] = i;
-    size[i] = 0;
-}
-
-// Union of each pixel with its right and lower neighbours: the larger root is hung under the smaller.
-static __global__ void k_speckle_union(const float* __restrict__ disp, int w, int h, float max_diff, int* parent, int* err) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= w || y >= h) return;
-    const int i = y * w + x;
-    const float d = disp[i];
-    if (!valid_disparity(d)) return;
-    const int nb[2] = {x + 1 < w ? i + 1 : -1, y + 1 < h ? i + w : -1};
-    for (int q = 0; q < 2; ++q) {
-        const int j = nb[q];
-        if (j < 0) continue;
-        const float dj = disp[j];
-        if (!valid_disparity(dj) || fabsf(__fsub_rn(dj, d)) > max_diff) continue;
-        uf_union(parent, i, j, err);
+// Speckle regions: valid pixels, linked when their disparities differ by at most max_diff.
+struct SpeckleConn {
+    const float* disp;
+    int w;
+    float max_diff;
+    __device__ __forceinline__ bool active(int x, int y) const { return valid_disparity(disp[static_cast<size_t>(y) * w + x]); }
+    __device__ __forceinline__ bool link(int x, int y, int x2, int y2) const {
+        const float d = disp[static_cast<size_t>(y) * w + x], dj = disp[static_cast<size_t>(y2) * w + x2];
+        return valid_disparity(dj) && !(fabsf(__fsub_rn(dj, d)) > max_diff);
     }
-}
+};
 
 // Component sizes once every union has landed. A find returns the true root however other threads halve
 // paths meanwhile, so the root is found again where it is used rather than stored in parent[]. Lanes of a

@@ -89,6 +89,14 @@ def test_find_blobs_bit_exact(cuda, port, params):
         big = np.full((300, 400), 255, np.uint8)                     # one huge component with holes
         big[::7, ::11] = 0
         imgs.append(big)
+        # near the percolation threshold: long, branching components across many 32 x 16 tiles and corners
+        rng = np.random.default_rng(11)
+        imgs.append(np.where(rng.random((203, 333)) < 0.58, 255, 0).astype(np.uint8))
+        corners = np.zeros((97, 161), np.uint8)                      # 2 x 2 squares on every tile corner
+        for y in range(15, 96, 16):
+            for x in range(31, 160, 32):
+                corners[y:y + 2, x:x + 2] = 200
+        imgs.append(corners)
         for k, img in enumerate(imgs):
             got, found = s.find_blobs(img)
             want, n = port.blob_candidates(img, bp)
