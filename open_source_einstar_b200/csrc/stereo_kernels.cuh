@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(256) k_costs(CostArgs a) {
 // aligned 128-bit load (u32 census). Thread t of a pixel writes the bytes of disparities 4t..4t+3, so
 // a warp stores whole 128-byte lines. Columns outside the right row give invalid_cost
 // (stereo.cpp:366-377).
-constexpr int kCostTile = 64;
+constexpr int kCostTile = 256;
 
 // Words per shifted copy (a multiple of 4, so that every copy starts 16-byte aligned).
 __host__ __device__ constexpr int cost_tile_copy_words(int dp) { return (kCostTile + dp + 3 + 3) / 4 * 4; }
@@ -121,6 +121,8 @@ __device__ __forceinline__ void cost_tile_body(const CostArgs& a, int b, CW* sm)
     const int t = threadIdx.x % tp, pi = threadIdx.x / tp;
     if (pi >= ppp) return;
     const uint32_t inv = static_cast<uint32_t>(a.invalid_cost);
+    // Interior tiles: every right column of the window inside the row, no per-cost range test.
+    const bool interior = r0 >= 0 && r0 + nr <= a.w;
     for (int px = pi; px < nx; px += ppp) {
         const CW vl = sl[px];
         const int g = px + a.dp - 4 - 4 * t;  // window slot of disparity 4t + 3; slot g + 3 - j is disparity 4t + j
@@ -134,12 +136,17 @@ __device__ __forceinline__ void cost_tile_body(const CostArgs& a, int b, CW* sm)
             for (int j = 0; j < 4; ++j) wv[j] = sm[g + j];
         }
         uint32_t word = 0;
+        if (interior) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {  // byte j: disparity 4t + j, right column r0 + g + 3 - j
-            const int xr = r0 + g + 3 - j;
-            const uint32_t cst = static_cast<unsigned>(xr) < static_cast<unsigned>(a.w)
-                                     ? static_cast<uint32_t>(popcount_word<CW>(vl ^ wv[3 - j])) : inv;
-            word |= cst << (8 * j);
+            for (int j = 0; j < 4; ++j) word |= static_cast<uint32_t>(popcount_word<CW>(vl ^ wv[3 - j])) << (8 * j);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {  // byte j: disparity 4t + j, right column r0 + g + 3 - j
+                const int xr = r0 + g + 3 - j;
+                const uint32_t cst = static_cast<unsigned>(xr) < static_cast<unsigned>(a.w)
+                                         ? static_cast<uint32_t>(popcount_word<CW>(vl ^ wv[3 - j])) : inv;
+                word |= cst << (8 * j);
+            }
         }
         *reinterpret_cast<uint32_t*>(a.costs + (static_cast<size_t>(y) * a.w + x0 + px) * a.dp + 4 * t) = word;
     }
