@@ -448,6 +448,7 @@ __device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
         padb[r] = ka + 1 >= a.nd ? kEmpty : 0u;
         padh[r] = (pada[r] & 0xFFFFu) | (padb[r] & 0xFFFF0000u);
     }
+    const bool unpadded = a.nd == SEG * NV;  // every lane slot is a real disparity
     // Double buffer: the next pixel's chunks are in flight while this one is reduced.
     uint32_t nxt[NDIRS][VW];
     auto fetch = [&](int xb) {
@@ -495,15 +496,27 @@ __device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
         uint32_t key, second;
         if (__all_sync(kFull, live && lo == 0 && hi == a.nd)) {
             // Interior pixels (every disparity < nd matches a column of the right row): no per-element
-            // range tests; padding keys are all ones and take part in nothing.
+            // range tests; padding keys are all ones and take part in nothing. Without padding (nd fills
+            // the lane slabs) the padding masks and tests drop out.
             uint32_t kmin = kEmpty;
+            if (unpadded) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const uint32_t key_a = prmt(kk[r], tot[r], 0x5410) | pada[r];  // (cost_a << 16) | ka
-                const uint32_t key_b = prmt(kk[r], tot[r], 0x7632) | padb[r];  // (cost_b << 16) | ka + 1
-                kmin = min(kmin, min(key_a, key_b));
-                if (key_a != kEmpty) atomicMin(&rkey[rbase - 2 * r], key_a);
-                if (key_b != kEmpty) atomicMin(&rkey[rbase - 2 * r - 1], key_b);
+                for (int r = 0; r < R; ++r) {
+                    const uint32_t key_a = prmt(kk[r], tot[r], 0x5410);  // (cost_a << 16) | ka
+                    const uint32_t key_b = prmt(kk[r], tot[r], 0x7632);  // (cost_b << 16) | ka + 1
+                    kmin = min(kmin, min(key_a, key_b));
+                    atomicMin(&rkey[rbase - 2 * r], key_a);
+                    atomicMin(&rkey[rbase - 2 * r - 1], key_b);
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const uint32_t key_a = prmt(kk[r], tot[r], 0x5410) | pada[r];
+                    const uint32_t key_b = prmt(kk[r], tot[r], 0x7632) | padb[r];
+                    kmin = min(kmin, min(key_a, key_b));
+                    if (key_a != kEmpty) atomicMin(&rkey[rbase - 2 * r], key_a);
+                    if (key_b != kEmpty) atomicMin(&rkey[rbase - 2 * r - 1], key_b);
+                }
             }
             key = seg_min<SEG>(kmin, seg);
             const int bk = static_cast<int>(key & 0xFFFFu);
@@ -514,7 +527,7 @@ __device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
                 // disparities within one of bk are not the second minimum (stereo.cpp:420-424)
                 const uint32_t ex = (static_cast<unsigned>(ka - bk + 1) <= 2u ? 0x0000FFFFu : 0u) |
                                     (static_cast<unsigned>(ka - bk + 2) <= 2u ? 0xFFFF0000u : 0u);
-                m2 = vmin2(m2, tot[r] | padh[r] | ex);
+                m2 = vmin2(m2, tot[r] | (unpadded ? 0u : padh[r]) | ex);
             }
             second = seg_min<SEG>(hmin2(m2), seg);
         } else {
