@@ -84,8 +84,43 @@ int main(int argc, char** argv) {
     if (!(*s)->set_blob_params({})) bad = 1;
     std::uint32_t found = 0;
     if (auto b = (*s)->find_blobs(l, &found); !b || b->size() != std::min<std::uint32_t>(found, 1024)) bad = 1;
-        // compute_raw before set_rectification: invalid_argument (metal_stereo.cpp:343)
+    // compute_raw before set_rectification: invalid_argument (metal_stereo.cpp:343)
     if (auto res = (*s)->compute_raw(l, r); res || res.error().code != depth_cuda::Errc::invalid_argument) bad = 1;
+    // the frontend's call (identity remap tables at the stereo size): compute_frame gives compute_raw's
+    // disparity, and its marker candidates are find_blobs' of each raw image
+    depth_cuda::RemapTable id{w, h, std::vector<float>(n), std::vector<float>(n)};
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            id.map_x[static_cast<std::size_t>(y) * w + x] = static_cast<float>(x);
+            id.map_y[static_cast<std::size_t>(y) * w + x] = static_cast<float>(y);
+        }
+    if (!(*s)->set_rectification(id, id, w, h)) bad = 1;
+    int callbacks = 0;
+    depth_cuda::FrameRequest req;
+    req.marker_blobs = true;
+    req.on_blobs = [&](const std::array<std::vector<depth_cuda::BlobBox>, 2>&) { ++callbacks; };
+    auto plain = (*s)->compute_raw(l, r);
+    auto frame = (*s)->compute_frame(l, r, req);
+    if (!plain || !frame || callbacks != 1) {
+        std::fprintf(stderr, "compute_frame failed or on_blobs not called once\n");
+        bad = 1;
+    } else {
+        if (std::memcmp(plain->disparity.data(), frame->disparity.data(), n * sizeof(float)) != 0) {
+            std::fprintf(stderr, "compute_frame disparity differs from compute_raw's\n");
+            bad = 1;
+        }
+        auto bl = (*s)->find_blobs(l), br = (*s)->find_blobs(r);
+        if (!bl || !br || bl->size() != frame->blobs[0].size() || br->size() != frame->blobs[1].size()) {
+            std::fprintf(stderr, "compute_frame blob counts differ from find_blobs'\n");
+            bad = 1;
+        }
+        else
+            for (int side = 0; side < 2; ++side) {
+                const auto& want = side == 0 ? *bl : *br;
+                if (!want.empty() && std::memcmp(want.data(), frame->blobs[side].data(), want.size() * sizeof(depth_cuda::BlobBox)) != 0)
+                    bad = 1;
+            }
+    }
     std::printf(bad ? "FAIL\n" : "OK\n");
     return bad;
 }
