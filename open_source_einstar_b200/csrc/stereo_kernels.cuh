@@ -13,6 +13,8 @@
 // them into FMAs, which the reference's separately rounded x86 arithmetic does not do.
 #pragma once
 
+#include <type_traits>
+
 #include <cstdint>
 #include <climits>
 
@@ -331,6 +333,10 @@ __device__ __forceinline__ void paths_body(const PathArgs& a, const int* p2, int
     if (len > 0) store(0, prev);
 
     int x = x0, y = y0;
+    // The step loop twice: with the padding masks, and without them for warps none of whose lanes has
+    // padding (predicated-off instructions would still take issue slots on every step).
+    auto steps = [&](auto pad_tag) {
+    constexpr bool PAD = decltype(pad_tag)::value;
     for (int base = 1; base < nsteps; base += PF) {
 #pragma unroll
         for (int u = 0; u < PF; ++u) {
@@ -359,7 +365,7 @@ __device__ __forceinline__ void paths_body(const PathArgs& a, const int* p2, int
                 if (a.slant) m = vmin2(m, vmin2(lower, upper));
                 const uint32_t best = vmin2(vmin2(vadd2(m, P12), prev[r]), jump2);
                 uint32_t L = vadd2(vadd2(best, c[r]), negpm);
-                if (any_pad) L = (L & ~pad[r]) | (INF2 & pad[r]);
+                if constexpr (PAD) L = (L & ~pad[r]) | (INF2 & pad[r]);
                 cur[r] = L;
                 lmin = vmin2(lmin, L);
             }
@@ -369,6 +375,9 @@ __device__ __forceinline__ void paths_body(const PathArgs& a, const int* p2, int
             if (s < len) store(s, cur);
         }
     }
+    };
+    if (__any_sync(kFull, any_pad)) steps(std::integral_constant<bool, true>{});
+    else steps(std::integral_constant<bool, false>{});
 }
 
 template <int R, int SEG, typename CW, typename ST, bool MAT, int PF>
