@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256) kb_paths(const PathArgs* __restrict__ arg
 }
 
 template <int R, int SEG, typename ST, int NDIRS>
-__global__ void __launch_bounds__(256) kb_wta(const WtaArgs* __restrict__ args, const int* __restrict__ pairs,
+__global__ void __launch_bounds__(256, sizeof(ST) == 1 && NDIRS == 4 ? 4 : 1) kb_wta(const WtaArgs* __restrict__ args, const int* __restrict__ pairs,
                                               const int* __restrict__ prefix, const int* __restrict__ gx, int n, int total) {
     __shared__ WtaArgs sa;
     int cur = -1;

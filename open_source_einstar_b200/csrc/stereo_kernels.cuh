@@ -607,7 +607,7 @@ __device__ __forceinline__ void wta_body(const WtaArgs& a, int bx) {
 }
 
 template <int R, int SEG, typename ST, int NDIRS>
-__global__ void __launch_bounds__(256) k_wta(WtaArgs a) {
+__global__ void __launch_bounds__(256, sizeof(ST) == 1 && NDIRS == 4 ? 4 : 1) k_wta(WtaArgs a) {
     wta_body<R, SEG, ST, NDIRS>(a, blockIdx.x);
 }
 
