@@ -167,21 +167,16 @@ __device__ __forceinline__ void post_body(const PostArgs& a, int bx, int by) {
     float d = __ldg(a.disp + i);
     if (a.median && valid_disparity(d)) {
         float v[9];
-        int n = 0;
+#pragma unroll
         for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
             for (int dx = -1; dx <= 1; ++dx) {
                 const int xx = x + dx, yy = y + dy;
-                if (xx < 0 || yy < 0 || xx >= a.w || yy >= a.h) continue;
-                const float q = __ldg(a.disp + static_cast<size_t>(yy) * a.w + xx);
-                if (!valid_disparity(q)) continue;
-                int p = n++;
-                while (p > 0 && v[p - 1] > q) {
-                    v[p] = v[p - 1];
-                    --p;
-                }
-                v[p] = q;
+                const bool in = xx >= 0 && yy >= 0 && xx < a.w && yy < a.h;
+                v[(dy + 1) * 3 + dx + 1] = in ? __ldg(a.disp + static_cast<size_t>(yy) * a.w + xx) : kInvalid;
             }
-        d = v[n / 2];
+        int n;
+        d = median_of_valid9(v, n);
     }
     const bool ok = valid_disparity(d);
     if (a.out_disp) a.out_disp[i] = d;

@@ -34,21 +34,16 @@ static __global__ void k_median3(const float* __restrict__ in, int w, int h, flo
     float d = in[i];
     if (valid_disparity(d)) {
         float v[9];
-        int n = 0;
+#pragma unroll
         for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
             for (int dx = -1; dx <= 1; ++dx) {
                 const int xx = x + dx, yy = y + dy;
-                if (xx < 0 || yy < 0 || xx >= w || yy >= h) continue;
-                const float q = in[static_cast<size_t>(yy) * w + xx];
-                if (!valid_disparity(q)) continue;
-                int p = n++;
-                while (p > 0 && v[p - 1] > q) {
-                    v[p] = v[p - 1];
-                    --p;
-                }
-                v[p] = q;
+                const bool inside = xx >= 0 && yy >= 0 && xx < w && yy < h;
+                v[(dy + 1) * 3 + dx + 1] = inside ? in[static_cast<size_t>(yy) * w + xx] : kInvalid;
             }
-        d = v[n / 2];
+        int n;
+        d = median_of_valid9(v, n);
     } else {
         d = kInvalid;
     }
@@ -460,21 +455,17 @@ static __global__ void k_filter_spikes(const float* __restrict__ in, int w, int 
     float res = d;
     if (valid_disparity(d)) {
         float v[9];
-        int n = 0;
+#pragma unroll
         for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
             for (int dx = -1; dx <= 1; ++dx) {
                 const int xx = x + dx, yy = y + dy;
-                if (xx < 0 || yy < 0 || xx >= w || yy >= h) continue;
-                const float q = in[static_cast<size_t>(yy) * w + xx];
-                if (!valid_disparity(q)) continue;
-                int p = n++;
-                while (p > 0 && v[p - 1] > q) {
-                    v[p] = v[p - 1];
-                    --p;
-                }
-                v[p] = q;
+                const bool inside = xx >= 0 && yy >= 0 && xx < w && yy < h;
+                v[(dy + 1) * 3 + dx + 1] = inside ? in[static_cast<size_t>(yy) * w + xx] : kInvalid;
             }
-        if (n >= 3 && fabsf(__fsub_rn(d, v[n / 2])) > threshold) res = kInvalid;
+        int n;
+        const float med = median_of_valid9(v, n);
+        if (n >= 3 && fabsf(__fsub_rn(d, med)) > threshold) res = kInvalid;
     }
     out[i] = res;
 }

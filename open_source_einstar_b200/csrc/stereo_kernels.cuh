@@ -29,6 +29,36 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 
 __host__ __device__ inline bool valid_disparity(float d) { return d > -1.0e8f; }  // stereo.hpp:24
 
+// The median of the valid values of a 3x3 neighbourhood as median3 / the spike filter take it
+// (stereo.cpp:129-147, 305-325): element n/2 of the n valid values in ascending order. Invalid values become
+// +inf and sink to the end of a 25-comparator sorting network over the nine values, all in registers (an
+// insertion sort into an array indexed at run time lives in local memory). Returns n through `count`.
+__device__ __forceinline__ float median_of_valid9(float (&v)[9], int& count) {
+    int n = 0;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        const bool ok = valid_disparity(v[k]);
+        n += ok;
+        v[k] = ok ? v[k] : __int_as_float(0x7F800000);
+    }
+#define DSK_CE(i, j)                                                 \
+    {                                                                \
+        const float lo_ = fminf(v[i], v[j]), hi_ = fmaxf(v[i], v[j]); \
+        v[i] = lo_;                                                  \
+        v[j] = hi_;                                                  \
+    }
+    DSK_CE(0, 1) DSK_CE(3, 4) DSK_CE(6, 7) DSK_CE(1, 2) DSK_CE(4, 5) DSK_CE(7, 8) DSK_CE(0, 1) DSK_CE(3, 4) DSK_CE(6, 7)
+    DSK_CE(0, 3) DSK_CE(3, 6) DSK_CE(0, 3) DSK_CE(1, 4) DSK_CE(4, 7) DSK_CE(1, 4) DSK_CE(2, 5) DSK_CE(5, 8) DSK_CE(2, 5)
+    DSK_CE(1, 3) DSK_CE(5, 7) DSK_CE(2, 6) DSK_CE(4, 6) DSK_CE(2, 4) DSK_CE(2, 3) DSK_CE(5, 6)
+#undef DSK_CE
+    const int m = n / 2;
+    float r = v[0];
+#pragma unroll
+    for (int k = 1; k < 9; ++k) r = m == k ? v[k] : r;
+    count = n;
+    return r;
+}
+
 // Path directions in the reference's order (stereo.cpp:387-388).
 static __constant__ int c_dir_dx[8] = {1, -1, 0, 0, 1, -1, 1, -1};
 static __constant__ int c_dir_dy[8] = {0, 0, 1, -1, 1, -1, -1, 1};
