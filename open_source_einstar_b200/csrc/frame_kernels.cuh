@@ -46,9 +46,10 @@ __device__ __forceinline__ void rectify_body(const RectifyArgs& a, int bx, int b
     const int y = by * blockDim.y + threadIdx.y;
     const int side = bz;
     if (x4 >= a.out_w || y >= a.out_h) return;
-    const uint8_t* src = a.raw[side];
-    const float* mx = a.map_x[side];
-    const float* my = a.map_y[side];
+    // (selected, not indexed: a run-time index into the argument's arrays would copy them to local memory)
+    const uint8_t* src = side ? a.raw[1] : a.raw[0];
+    const float* mx = side ? a.map_x[1] : a.map_x[0];
+    const float* my = side ? a.map_y[1] : a.map_y[0];
     const bool full = x4 + 4 <= a.out_w;
     uint32_t v[4] = {0u, 0u, 0u, 0u};
     if (!a.half) {
@@ -76,7 +77,7 @@ __device__ __forceinline__ void rectify_body(const RectifyArgs& a, int bx, int b
             v[j] = (acc + 2u) / 4u;
         }
     }
-    uint8_t* out = a.out[side] + static_cast<size_t>(y) * a.out_w + x4;
+    uint8_t* out = (side ? a.out[1] : a.out[0]) + static_cast<size_t>(y) * a.out_w + x4;
     if (full && (a.out_w & 3) == 0) {
         *reinterpret_cast<uint32_t*>(out) = v[0] | (v[1] << 8) | (v[2] << 16) | (v[3] << 24);
     } else {
@@ -105,7 +106,7 @@ template <typename W>
 __device__ __forceinline__ void census_body(const CensusArgs& a, int bx, int by, int bz) {
     __shared__ uint8_t tile[8 + 2 * kCensusMaxRy][32 + 2 * kCensusMaxRx];
     const int x0 = bx * 32, y0 = by * 8;
-    const uint8_t* img = a.img[bz];
+    const uint8_t* img = bz ? a.img[1] : a.img[0];  // selected, not indexed (see rectify_body)
     const int tw = 32 + 2 * a.rx, th = 8 + 2 * a.ry;
     const int tid = threadIdx.y * 32 + threadIdx.x;
     __syncthreads();  // the previous virtual block's readers are done
@@ -135,7 +136,7 @@ __device__ __forceinline__ void census_body(const CensusArgs& a, int bx, int by,
                 }
         }
     }
-    static_cast<W*>(a.out[bz])[static_cast<size_t>(y) * a.pitch + x] = word;
+    static_cast<W*>(bz ? a.out[1] : a.out[0])[static_cast<size_t>(y) * a.pitch + x] = word;
 }
 
 template <typename W>
