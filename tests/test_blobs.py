@@ -97,6 +97,8 @@ def test_find_blobs_bit_exact(cuda, port, params):
             for x in range(31, 160, 32):
                 corners[y:y + 2, x:x + 2] = 200
         imgs.append(corners)
+        for hh, ww in ((5, 7), (17, 33), (16, 32), (31, 65)):        # smaller than a tile; one border row / column
+            imgs.append(np.where(rng.random((hh, ww)) < 0.6, 230, 10).astype(np.uint8))
         for k, img in enumerate(imgs):
             got, found = s.find_blobs(img)
             want, n = port.blob_candidates(img, bp)
