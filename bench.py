@@ -321,8 +321,8 @@ def run_batch64(args, world, rank, local):
     for pr in pairs:
         h, w = pr.left.shape
         sp = StereoParams(sgm=SgmParams(min_disparity=pr.min_disparity, num_disparities=pr.num_disparities))
-        kcfg = tuner.tune(FrameKind.of(w, h, sp))                  # per-frame path (fused pairs allowed)
-        bcfg = tuner.tune(FrameKind.of(w, h, sp), fused_ok=False)  # batched path
+        kcfg = tuner.tune(FrameKind.of(w, h, sp))              # per-frame path
+        bcfg = tuner.tune(FrameKind.of(w, h, sp), batch=True)  # batched path
         geom = RectifiedGeometry(pr.f, 0, 0, pr.baseline, 0.0)
         descs.append(PairDesc(w, h, sp, geometry=geom, kernel=bcfg))
         s = CudaStereo.create(sp, w, h)
@@ -428,7 +428,7 @@ def run_offline(args, world, rank, local):
     sp = StereoParams(sgm=SgmParams(min_disparity=rec.min_disparity, num_disparities=D_, eight_paths=True),
                       wide_costs=True)
     geom = RectifiedGeometry(rec.rect.f, 0, 0, rec.rect.baseline, rec.rect.cx_offset)
-    kernel = Autotuner().tune(FrameKind.of(W_, H_, sp), fused_ok=False)
+    kernel = Autotuner().tune(FrameKind.of(W_, H_, sp), batch=True)
     out_u16 = pinned_empty((n, H_, W_), np.uint16)
     out_depth = pinned_empty((n, H_, W_), np.float32)
     with OfflineRedepth(W_, H_, sp, rec.maps, (W_, H_), geom, batch_size=args.offline_batch, kernel=kernel) as off:

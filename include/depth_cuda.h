@@ -191,9 +191,12 @@ DS_API uint64_t ds_kernel_launches(void);
  * create, metal_stereo.cpp:178-189). A scanline is run by `lanes_per_line` lanes (8, 16 or 32) holding
  * 2*regs_per_lane disparities each, so lanes_per_line * 2 * regs_per_lane >= num_disparities (the WTA
  * picks its own split of the same disparities). Supported: 8 lanes with regs 4, 6, 8; 16 lanes with
- * regs 1..4; 32 lanes with regs 1, 2, 3, 4, 6, 8 (fused pairs: 16 or 32 lanes). materialize_costs: write the
- * matching-cost volume once instead of recomputing costs from the census in every direction. Results are
- * identical for every configuration; only speed differs (the autotuner chooses). */
+ * regs 1..4; 32 lanes with regs 1, 2, 3, 4, 6, 8. materialize_costs: write the matching-cost volume once
+ * instead of recomputing costs from the census in every direction. fused_pairs selects the sweep kernels
+ * instead: the vertical path pair, then the horizontal pair with the WTA and the L-R check (two launches
+ * per frame, 6 bytes of volume traffic per pixel and disparity). They need 4 paths, census windows of at
+ * most 32 neighbours, 2 (window + P2) <= 255, and 4 or 8 lanes per line with regs 6 or 8 (D <= 128).
+ * Results are identical for every configuration; only speed differs (the autotuner chooses). */
 typedef struct ds_kernel_config {
     int regs_per_lane;
     int lanes_per_line;
@@ -201,9 +204,8 @@ typedef struct ds_kernel_config {
     int path_warps_per_block; /* 1..8 */
     int wta_threads;          /* multiple of 32, 32..256 */
     int prefetch_steps;       /* 4 or 8: steps of inputs each scanline keeps in flight */
-    int fused_pairs;          /* 4 paths only: opposite directions as meet-in-the-middle warp pairs, WTA fused
-                               * into the horizontal pair (path_warps_per_block <= 4 per direction) */
-    int horz_warps_per_block; /* fused: warps per direction of the horizontal pair kernel, 1..4 */
+    int fused_pairs;          /* the sweep kernels (see above); block shapes are fixed */
+    int horz_warps_per_block; /* unused by the sweep kernels (kept for layout) */
 } ds_kernel_config;
 DS_API int ds_set_kernel_config(ds_handle* handle, const ds_kernel_config* config);
 DS_API int ds_get_kernel_config(const ds_handle* handle, ds_kernel_config* config);
@@ -220,7 +222,7 @@ typedef struct ds_pair_desc {
     int have_geometry;         /* 1: depth output with `geometry` and the depth gates */
     ds_geometry geometry;
     float min_depth_mm, max_depth_mm;
-    ds_kernel_config kernel;   /* regs_per_lane 0: the library's default; fused_pairs is ignored */
+    ds_kernel_config kernel;   /* regs_per_lane 0: the library's default */
 } ds_pair_desc;
 
 typedef struct ds_batch ds_batch;

@@ -14,12 +14,17 @@ The knobs (ds_kernel_config in include/depth_cuda.h):
   from the census words in every direction.
 - prefetch_steps: steps of cost / census input kept in flight per scanline (4 or 8).
 - wta_threads: threads per winner-takes-all block.
-- fused_pairs (per-frame path, 4 directions): the two meet-in-the-middle pair kernels.
+- fused_pairs (4 directions): the two sweep kernels instead of cost / path / WTA kernels: the vertical path
+  pair, then the horizontal pair with the WTA and the L-R check. They need byte pair sums
+  (2 (window + P2) <= 255), census windows of at most 32 neighbours and D <= 128, with 4 or 8 lanes per
+  line of 12 or 16 disparities; their block shapes are fixed.
 
-The search is staged: tile shape x materialisation, then paths per block x prefetch, then the WTA
-block. That is about 16 timed configurations instead of the full product.
+The search is staged: tile shape x materialisation (and the sweep shapes), then paths per block x
+prefetch, then the WTA block. That is about 16 timed configurations instead of the full product. The
+per-frame path and the batched path are tuned separately (a batch keeps many frames in flight, so its
+best kernels can differ).
 
-    python -m open_source_einstar_b200.autotune 1280x1024:128 640x512:64 --write
+    python -m open_source_einstar_b200.autotune 1280x1024:128 640x512:64 --batch --write
 """
 from __future__ import annotations
 
@@ -33,6 +38,7 @@ import numpy as np
 
 PACKAGE_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "b200.json")
 SUPPORTED = {8: (4, 6, 8), 16: (1, 2, 3, 4), 32: (1, 2, 3, 4, 6, 8)}
+SWEEP_SHAPES = {4: (6, 8), 8: (6, 8)}  # lanes per line -> registers per lane of the sweep kernels
 DEFAULT = {"path_warps_per_block": 4, "wta_threads": 256, "prefetch_steps": 8, "fused_pairs": 0,
            "horz_warps_per_block": 4}
 
@@ -45,6 +51,7 @@ class FrameKind:
     eight_paths: bool = False
     wide: bool = False          # u16 path values (window + P2 > 255 or forced)
     census_window: int = 25
+    byte_pair_sums: bool = True  # 2 (window + P2) <= 255 (not part of the key: it follows from the parameters)
 
     def key(self, device: str) -> str:
         return (f"{device}|{self.width}x{self.height}|D{self.num_disparities}|P{8 if self.eight_paths else 4}|"
@@ -54,8 +61,14 @@ class FrameKind:
     def of(width: int, height: int, params) -> "FrameKind":
         s = params.sgm
         window = (2 * s.census_radius_x + 1) * (2 * s.census_radius_y + 1)
-        return FrameKind(int(width), int(height), int(s.num_disparities), bool(s.eight_paths),
-                         bool(params.wide_costs or window + s.p2 > 255), window)
+        wide = bool(params.wide_costs or window + s.p2 > 255)
+        return FrameKind(int(width), int(height), int(s.num_disparities), bool(s.eight_paths), wide, window,
+                         not wide and 2 * (window + s.p2) <= 255)
+
+    def sweep_fit(self) -> bool:
+        """Whether the sweep kernels can run this kind of frame (the library's own check, sweep_unfit)."""
+        return (not self.eight_paths and self.byte_pair_sums and self.census_window - 1 <= 32
+                and self.num_disparities <= 128)
 
 
 def tile_shapes(num_disparities: int) -> list[tuple[int, int]]:
@@ -68,23 +81,31 @@ def tile_shapes(num_disparities: int) -> list[tuple[int, int]]:
     return out
 
 
+def sweep_shapes(num_disparities: int) -> list[tuple[int, int]]:
+    """(R, SEG) of the sweep kernels with the fewest padded disparities for each SEG (SEG*2R >= D)."""
+    out = []
+    for seg, rs in SWEEP_SHAPES.items():
+        fit = [r for r in rs if seg * 2 * r >= num_disparities]
+        if fit:
+            out.append((min(fit), seg))
+    return out
+
+
 def stage_candidates(kind: FrameKind, stage: int, best: dict | None = None, fused_ok: bool = True) -> list[dict]:
-    """Candidates of one search stage (1: tile x materialisation [x fused], 2: warps x prefetch, 3: WTA)."""
+    """Candidates of one search stage (1: tile x materialisation, and the sweep shapes; 2: warps x prefetch;
+    3: WTA). fused_ok=False leaves the sweep kernels out."""
     if stage == 1:
         c = []
         for r, seg in tile_shapes(kind.num_disparities):
             for mat in (1, 0):
                 c.append({"regs_per_lane": r, "lanes_per_line": seg, "materialize_costs": mat, **DEFAULT})
-            if fused_ok and not kind.eight_paths and seg != 8:
-                c.append({"regs_per_lane": r, "lanes_per_line": seg, "materialize_costs": 0, **DEFAULT,
-                          "fused_pairs": 1})
+        if fused_ok and kind.sweep_fit():
+            for r, seg in sweep_shapes(kind.num_disparities):
+                c.append({"regs_per_lane": r, "lanes_per_line": seg, "materialize_costs": 0, **DEFAULT, "fused_pairs": 1})
         return c
     assert best is not None
     if best.get("fused_pairs"):
-        if stage == 2:
-            return [{**best, "path_warps_per_block": pw, "horz_warps_per_block": hw}
-                    for pw in (2, 4, 8) for hw in (2, 4)]
-        return [best]
+        return [best]  # the sweep kernels have fixed block shapes
     if stage == 2:
         return [{**best, "path_warps_per_block": pw, "prefetch_steps": pf} for pw in (1, 2, 4, 8) for pf in (4, 8)]
     return [{**best, "wta_threads": t} for t in (128, 256)]
@@ -139,12 +160,11 @@ class Autotuner:
         return torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
 
     @staticmethod
-    def _key(kind: FrameKind, device: str, fused_ok: bool) -> str:
-        # the batched path has no fused pair kernels: it is tuned separately
-        return kind.key(device) + ("" if fused_ok else "|batch")
+    def _key(kind: FrameKind, device: str, batch: bool) -> str:
+        return kind.key(device) + ("|batch" if batch else "")  # the batched path is tuned separately
 
-    def lookup(self, kind: FrameKind, device: str | None = None, fused_ok: bool = True) -> dict | None:
-        e = self.table.get(self._key(kind, device or self.device_name(), fused_ok))
+    def lookup(self, kind: FrameKind, device: str | None = None, batch: bool = False) -> dict | None:
+        e = self.table.get(self._key(kind, device or self.device_name(), batch))
         return dict(e["config"]) if e else None
 
     def save(self, path: str | None = None) -> str:
@@ -154,17 +174,18 @@ class Autotuner:
             json.dump({"format": 1, "entries": self.table}, f, indent=1, sort_keys=True)
         return path
 
-    def tune(self, kind: FrameKind, frames: int = 8, warmup: int = 2, force: bool = False, fused_ok: bool = True,
+    def tune(self, kind: FrameKind, frames: int = 8, warmup: int = 2, force: bool = False, batch: bool = False,
              params=None) -> dict:
-        """The fastest configuration for `kind` (timed on the current GPU unless already in the table)."""
+        """The fastest configuration for `kind` on the per-frame path (batch=False) or the batched path,
+        timed on the current GPU unless already in the table."""
         dev = self.device_name()
         if not force:
-            hit = self.lookup(kind, dev, fused_ok)
+            hit = self.lookup(kind, dev, batch)
             if hit:
                 return hit
-        time_fn = device_timer(kind, frames, warmup, params) if fused_ok else batch_timer(kind, warmup, params)
-        best, info = search(kind, time_fn, fused_ok)
-        self.table[self._key(kind, dev, fused_ok)] = {
+        time_fn = batch_timer(kind, warmup, params) if batch else device_timer(kind, frames, warmup, params)
+        best, info = search(kind, time_fn)
+        self.table[self._key(kind, dev, batch)] = {
             "config": best, "ms_per_frame": info["ms"],
             "trials": [[c, ms] for st in info["trials"].values() for c, ms in st]}
         return dict(best)
@@ -188,7 +209,7 @@ def tuned_config(width: int, height: int, params, batch: bool = False) -> dict |
     if _shared is None:
         _shared = Autotuner()
         _device = Autotuner.device_name()
-    return _shared.lookup(FrameKind.of(width, height, params), _device, fused_ok=not batch)
+    return _shared.lookup(FrameKind.of(width, height, params), _device, batch=batch)
 
 
 def apply(stereo, cfg: dict) -> None:
@@ -319,16 +340,16 @@ def main(argv=None) -> int:
     ap.add_argument("kinds", nargs="+", help="WxH:D[,p8][,u16] frame kinds, e.g. 1280x1024:128 1280x1024:256,p8,u16")
     ap.add_argument("--write", action="store_true", help="write the packaged table (tuning/b200.json)")
     ap.add_argument("--frames", type=int, default=8)
-    ap.add_argument("--batch", action="store_true", help="also tune for the batched path (no fused pair kernels)")
+    ap.add_argument("--batch", action="store_true", help="also tune for the batched path")
     args = ap.parse_args(argv)
     t = Autotuner(table_path=PACKAGE_TABLE if args.write else None, read_package_table=True)
     for ks in args.kinds:
         kind = _parse_kind(ks)
-        for fused_ok in ((True, False) if args.batch else (True,)):
+        for batch in ((False, True) if args.batch else (False,)):
             t0 = time.perf_counter()
-            cfg = t.tune(kind, frames=args.frames, force=True, fused_ok=fused_ok)
-            e = t.table[t._key(kind, t.device_name(), fused_ok)]
-            print(json.dumps({"kind": ks, "batch": not fused_ok, "config": cfg, "ms_per_frame": e["ms_per_frame"],
+            cfg = t.tune(kind, frames=args.frames, force=True, batch=batch)
+            e = t.table[t._key(kind, t.device_name(), batch)]
+            print(json.dumps({"kind": ks, "batch": batch, "config": cfg, "ms_per_frame": e["ms_per_frame"],
                               "tuning_s": time.perf_counter() - t0}), flush=True)
     if args.write:
         print("wrote", t.save(PACKAGE_TABLE))

@@ -16,7 +16,7 @@
 #include "batch_common.cuh"
 #include "dispatch.h"
 #include "frame_kernels.cuh"
-#include "fused_kernels.cuh"
+#include "sweep_kernels.cuh"
 #include "internal.h"
 #include "refine_kernels.cuh"
 #include "blob_kernels.cuh"
@@ -69,7 +69,7 @@ struct ds_handle {
     ds::KernelCfg cfg{};
     bool wide = false;      // u16 path values
     bool census64 = false;  // u64 census words
-    bool s16 = false;       // fused pairs: u16 vertical sums (2 (window + P2) > 255 or wide)
+    bool s16 = false;       // vertical pair sums need 16 bits (2 (window + P2) > 255 or wide): no sweep kernels
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
@@ -84,8 +84,12 @@ struct ds_handle {
     void* census_raw[2] = {nullptr, nullptr};
     int cpitch = 0, cguard = 0;
     size_t census_bytes = 0;                   // per image, guards included (capacity)
-    void* d_S = nullptr;                       // fused pairs: vertical sums and horizontal scratch, inside d_values
+    // Sweep kernels (cfg.fused), all inside d_values: vertical pair sums S and horizontal first-half values T
+    // (u8 slabs with guard rows), the row kernel's per-pixel WTA records and its right-WTA keys.
+    void* d_S = nullptr;
     void* d_T = nullptr;
+    uint2* d_rec = nullptr;
+    uint16_t* d_rk = nullptr;
     void* d_values = nullptr;
     size_t dir_stride = 0;
     size_t values_bytes = 0;
@@ -263,21 +267,18 @@ bool refines(const ds_stereo_params& p) {
     return p.pyramid_levels > 0 || p.detail_enabled || p.filter_occlusion || p.filter_spikes || p.speckle_max_region_size > 1;
 }
 
-constexpr size_t kMaxSmem = 227 * 1024;
-
-size_t horz_smem(const ds_handle* h, const ds::KernelCfg& c) {
-    return static_cast<size_t>(c.horz_warps) * (32 / c.seg) * h->w * 4 * dsk::kHorzWordsPerPixel;
-}
-
-dsk::FusedArgs fused_args(const ds_handle* h) {
+dsk::SweepArgs sweep_args(const ds_handle* h) {
     const auto& sg = h->p.sgm;
-    dsk::FusedArgs a{};
-    a.census_l = h->d_census[0];
-    a.census_r = h->d_census[1];
+    dsk::SweepArgs a{};
+    a.census_l = static_cast<const uint32_t*>(h->d_census[0]);
+    a.census_r = static_cast<const uint32_t*>(h->d_census[1]);
     a.cpitch = h->cpitch;
     a.guide = h->d_rect[0];
-    a.S = h->d_S;
-    a.T = h->d_T;
+    a.S = static_cast<uint8_t*>(h->d_S);
+    a.T = static_cast<uint8_t*>(h->d_T);
+    a.rec = h->d_rec;
+    a.rk = h->d_rk;
+    a.disp = h->d_disp_lr;
     a.w = h->w;
     a.h = h->h;
     a.nd = h->nd;
@@ -285,16 +286,26 @@ dsk::FusedArgs fused_args(const ds_handle* h) {
     a.min_disp = sg.min_disparity;
     a.p1 = sg.p1;
     a.invalid_cost = (2 * sg.census_radius_x + 1) * (2 * sg.census_radius_y + 1);
-    a.slant = sg.slant_steps ? 1 : 0;
+    a.uniqueness = sg.uniqueness;
+    a.subpixel = h->p.subpixel ? 1 : 0;
+    a.lr_max_diff = sg.lr_max_diff;
     for (int q = 0; q < 32; ++q) {
         const int p2 = sg.adaptive_p2 ? std::max(sg.p1 + 1, sg.p2 / (q + 1)) : sg.p2;
         a.p2_table2[q] = static_cast<uint32_t>(p2) * 0x00010001u;
     }
-    a.uniqueness = sg.uniqueness;
-    a.subpixel = h->p.subpixel ? 1 : 0;
-    a.lr_max_diff = sg.lr_max_diff;
-    a.disp = h->d_disp_lr;
     return a;
+}
+
+bool sweep_slant(const ds_handle* h) { return h->p.sgm.slant_steps != 0; }
+bool sweep_pad(const ds_handle* h) { return h->nd < h->dp; }
+
+// Why the sweep kernels cannot run this handle's frames ("" when they can).
+const char* sweep_unfit(const ds_handle* h, int R, int seg) {
+    if (h->ndirs != 4) return "the sweep kernels need 4 paths";
+    if (h->census64) return "the sweep kernels need census windows of at most 32 neighbours";
+    if (h->s16) return "the sweep kernels need 2 (window + P2) <= 255 (byte pair sums)";
+    if (!dsk::sweep_shape_ok(R, seg)) return "the sweep kernels need 6 or 8 registers per lane and 4 or 8 lanes per line";
+    return "";
 }
 
 // The materialised cost volume (nothing when the path kernels recompute costs from the census).
@@ -315,7 +326,7 @@ void launch_costs(ds_handle* h, cudaStream_t st) {
 
 void launch_paths(ds_handle* h, cudaStream_t st) {
     if (h->cfg.fused) {
-        DS_CUDA(ds::launch_vert(h->cfg, h->census64, h->s16, fused_args(h), st));
+        DS_CUDA(ds::launch_sweep_cols(h->cfg, sweep_slant(h), sweep_pad(h), sweep_args(h), st));
         ++g_launches;
         return;
     }
@@ -346,7 +357,7 @@ void launch_paths(ds_handle* h, cudaStream_t st) {
 
 void launch_wta(ds_handle* h, cudaStream_t st) {
     if (h->cfg.fused) {
-        DS_CUDA(ds::launch_horz(h->cfg, h->census64, h->s16, fused_args(h), horz_smem(h, h->cfg), st));
+        DS_CUDA(ds::launch_sweep_rows(h->cfg, sweep_slant(h), sweep_pad(h), sweep_args(h), st));
         ++g_launches;
         return;
     }
@@ -376,6 +387,33 @@ void free_counted(ds_handle* h, void*& p, size_t bytes) {
     }
 }
 
+// The sweep kernels' buffers inside the path-value volume: S and T slabs (u8 [y][x][dp] with kGuardRows guard
+// rows above and below), then the WTA records (8 bytes per pixel) and the right-WTA keys (2 x 2 bytes).
+size_t sweep_slab_bytes(const ds_handle* h) {
+    return (static_cast<size_t>(h->h + 2 * dsk::kGuardRows) * h->w * h->dp + 255) / 256 * 256;
+}
+size_t sweep_volume_bytes(const ds_handle* h) {
+    const size_t n = static_cast<size_t>(h->w) * h->h;
+    return 2 * sweep_slab_bytes(h) + (n * 8 + 255) / 256 * 256 + n * 4;
+}
+void bind_sweep_buffers(ds_handle* h) {
+    if (!h->cfg.fused || !h->d_values) {
+        h->d_S = h->d_T = nullptr;
+        h->d_rec = nullptr;
+        h->d_rk = nullptr;
+        return;
+    }
+    const size_t n = static_cast<size_t>(h->w) * h->h;
+    const size_t slab = sweep_slab_bytes(h), lead = static_cast<size_t>(dsk::kGuardRows) * h->w * h->dp;
+    uint8_t* base = static_cast<uint8_t*>(h->d_values);
+    h->d_S = base + lead;
+    h->d_T = base + slab + lead;
+    h->d_rec = reinterpret_cast<uint2*>(base + 2 * slab);
+    h->d_rk = reinterpret_cast<uint16_t*>(base + 2 * slab + (n * 8 + 255) / 256 * 256);
+}
+
+constexpr int kCensusSlack = 40;
+
 // (Re)allocates the buffers whose size depends on the kernel configuration. The census and the fused
 // slabs carry kGuardRows guard rows above and below (and the census guard columns) for the prefetches.
 void size_config_buffers(ds_handle* h) {
@@ -386,14 +424,16 @@ void size_config_buffers(ds_handle* h) {
     h->dir_stride = n * static_cast<size_t>(h->dp);
     {
         const int mind = h->p.sgm.min_disparity;
-        const int guard = (std::max(mind + h->dp, 0) + std::max(-mind, 0) + g + 4 + 3) / 4 * 4;
+        // + kCensusSlack: the column sweep kernel's lanes past the row end (a column group is up to 32 columns)
+        // and its 16-byte aligned loads read up to 36 words beyond the last real column's window.
+        const int guard = (std::max(mind + h->dp, 0) + std::max(-mind, 0) + g + kCensusSlack + 3) / 4 * 4;
         const int pitch = (h->w + 2 * guard + 3) / 4 * 4;
         const size_t cw = h->census64 ? 8 : 4;
         const size_t cb = static_cast<size_t>(h->h + 2 * g) * pitch * cw;
         if (cb > h->census_bytes) {  // capacity: a smaller layout reuses the buffers
             size_t cap = cb;
             if (h->any_min_disparity) {  // room for the guards of every min_disparity in [-512, 512]
-                const int gmax = (dsk::kMaxDisparities + h->dp + g + 4 + 3) / 4 * 4;
+                const int gmax = (dsk::kMaxDisparities + h->dp + g + kCensusSlack + 3) / 4 * 4;
                 cap = std::max(cap, static_cast<size_t>(h->h + 2 * g) * ((h->w + 2 * gmax + 3) / 4 * 4) * cw);
             }
             for (auto*& p : h->census_raw) free_counted(h, p, h->census_bytes);
@@ -406,15 +446,14 @@ void size_config_buffers(ds_handle* h) {
         for (int s = 0; s < 2; ++s)
             h->d_census[s] = static_cast<uint8_t*>(h->census_raw[s]) + (static_cast<size_t>(g) * pitch + guard) * cw;
     }
-    const size_t slab = static_cast<size_t>(h->h + 2 * g) * h->w * h->dp * (h->s16 ? 2 : 1);  // fused, bytes
-    const size_t vb = h->cfg.fused ? 2 * slab : h->dir_stride * h->ndirs * (h->wide ? 2 : 1);
+    const size_t vb = h->cfg.fused ? sweep_volume_bytes(h) : h->dir_stride * h->ndirs * (h->wide ? 2 : 1);
     const size_t cb = h->cfg.materialize && !h->cfg.fused ? n * static_cast<size_t>(h->dp) : 0;
-    if (h->external_volumes) {  // a batch binds shared volumes later (never the fused kernels)
+    if (h->external_volumes) {  // a batch or the request server binds shared volumes later
         h->values_bytes = vb;
         h->costs_bytes = cb;
         h->d_values = nullptr;
         h->d_costs = nullptr;
-        h->d_S = h->d_T = nullptr;
+        bind_sweep_buffers(h);
         return;
     }
     if (vb != h->values_bytes) {
@@ -427,13 +466,7 @@ void size_config_buffers(ds_handle* h) {
         h->d_values = h->alloc<uint8_t>(vb);
         h->values_bytes = vb;
     }
-    if (h->cfg.fused) {
-        const size_t lead = static_cast<size_t>(g) * h->w * h->dp * (h->s16 ? 2 : 1);
-        h->d_S = static_cast<uint8_t*>(h->d_values) + lead;
-        h->d_T = static_cast<uint8_t*>(h->d_values) + slab + lead;
-    } else {
-        h->d_S = h->d_T = nullptr;
-    }
+    bind_sweep_buffers(h);
     if (cb != h->costs_bytes) {
         if (h->d_costs) {
             cudaFree(h->d_costs);
@@ -916,12 +949,6 @@ cudaError_t launch_wta(const KernelCfg& cfg0, bool wide, const dsk::WtaArgs& a, 
 cudaError_t launch_costs(const KernelCfg& cfg, bool c64, const dsk::CostArgs& a, cudaStream_t st) {
     DS_BY_R(launch_costs, cfg, c64, a, st)
 }
-cudaError_t launch_vert(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, cudaStream_t st) {
-    DS_BY_R(launch_vert, cfg, c64, s16, a, st)
-}
-cudaError_t launch_horz(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, size_t smem, cudaStream_t st) {
-    DS_BY_R(launch_horz, cfg, c64, s16, a, smem, st)
-}
 cudaError_t launch_paths_batch(const KernelCfg& cfg, bool c64, bool wide, const dsk::PathArgs* args, const BatchGroupDev& g,
                                cudaStream_t st) {
     DS_BY_R(launch_paths_batch, cfg, c64, wide, args, g, st)
@@ -1047,13 +1074,9 @@ int create_handle(const ds_stereo_params* params, int width, int height, bool ex
         // Path values are at most window + P2 (the recurrence never lets best exceed min(prev) + P2).
         h->wide = params->wide_costs || window + params->sgm.p2 > 255;
         h->s16 = h->wide || 2 * (window + params->sgm.p2) > 255;
-        h->cfg.fused = false;  // the fused pairs are selectable (ds_set_kernel_config / autotuner)
+        h->cfg.fused = false;  // the sweep kernels are selectable (ds_set_kernel_config / autotuner)
         h->external_volumes = external_volumes;
         h->any_min_disparity = any_min_disparity;
-        if (h->ndirs == 4) {
-            const int rows_max = static_cast<int>(kMaxSmem / (static_cast<size_t>(width) * 4 * dsk::kHorzWordsPerPixel));
-            h->cfg.horz_warps = std::max(1, std::min(4, rows_max / (32 / h->cfg.seg)));
-        }
         DS_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
         DS_CUDA(cudaEventCreate(&h->ev0));
         DS_CUDA(cudaEventCreate(&h->ev1));
@@ -1132,6 +1155,7 @@ size_t volume_bytes(const ds_handle* h) { return (h->values_bytes + 255) / 256 *
 void bind_volumes(ds_handle* h, void* base) {
     h->d_values = base;
     h->d_costs = h->costs_bytes ? static_cast<uint8_t*>(base) + (h->values_bytes + 255) / 256 * 256 : nullptr;
+    bind_sweep_buffers(h);
 }
 
 int bind_rectification(ds_handle* h, float* const maps[4], int map_w, int map_h, int raw_w, int raw_h) {
@@ -1432,13 +1456,18 @@ DS_API int ds_debug_read(ds_handle* h, uint64_t* census_left, uint64_t* census_r
             void* vals = h->d_values;
             void* tmp = nullptr;
             cudaError_t e = cudaSuccess;
+            size_t stride = h->dir_stride;
+            int dp = h->dp;
             if (h->cfg.fused) {
-                // The fused pairs keep no per-direction values: recompute them with the per-direction kernel.
-                e = cudaMalloc(&tmp, h->dir_stride * h->ndirs * (h->wide ? 2 : 1));
+                // The sweep kernels keep no per-direction values: recompute them with the per-direction kernel
+                // in the library's default classic configuration.
+                ds::KernelCfg gc = default_cfg(h->nd);
+                gc.fused = false;
+                gc.materialize = false;
+                dp = gc.dp();
+                stride = n * static_cast<size_t>(dp);
+                e = cudaMalloc(&tmp, stride * h->ndirs * (h->wide ? 2 : 1));
                 if (e == cudaSuccess) {
-                    ds::KernelCfg gc = h->cfg;
-                    gc.fused = false;
-                    gc.materialize = false;
                     const auto& sg = h->p.sgm;
                     dsk::PathArgs pa{};
                     pa.census_l = h->d_census[0];
@@ -1446,11 +1475,11 @@ DS_API int ds_debug_read(ds_handle* h, uint64_t* census_left, uint64_t* census_r
                     pa.cpitch = h->cpitch;
                     pa.guide = h->d_rect[0];
                     pa.values = tmp;
-                    pa.dir_stride = h->dir_stride;
+                    pa.dir_stride = stride;
                     pa.w = h->w;
                     pa.h = h->h;
                     pa.nd = h->nd;
-                    pa.dp = h->dp;
+                    pa.dp = dp;
                     pa.min_disp = sg.min_disparity;
                     pa.p1 = sg.p1;
                     pa.invalid_cost = (2 * sg.census_radius_x + 1) * (2 * sg.census_radius_y + 1);
@@ -1460,7 +1489,7 @@ DS_API int ds_debug_read(ds_handle* h, uint64_t* census_left, uint64_t* census_r
                     vals = tmp;
                 }
             }
-            dsk::SumArgs a{vals, h->dir_stride, h->ndirs, h->w, h->h, h->nd, h->dp, d};
+            dsk::SumArgs a{vals, stride, h->ndirs, h->w, h->h, h->nd, dp, d};
             if (e == cudaSuccess) {
                 if (h->wide) dsk::k_debug_sums<uint16_t><<<1024, 256, 0, h->stream>>>(a);
                 else dsk::k_debug_sums<uint8_t><<<1024, 256, 0, h->stream>>>(a);
@@ -1523,24 +1552,18 @@ DS_API int ds_set_kernel_config(ds_handle* h, const ds_kernel_config* c) {
         if (rc != DS_OK) h->err = h->sgm->err;
         return rc;
     }
-    if (!ds::cfg_supported(c->regs_per_lane, c->lanes_per_line))
+    if (c->fused_pairs) {
+        const char* why = sweep_unfit(h, c->regs_per_lane, c->lanes_per_line);
+        if (*why) return h->fail(DS_INVALID_ARGUMENT, why);
+    } else if (!ds::cfg_supported(c->regs_per_lane, c->lanes_per_line)) {
         return h->fail(DS_INVALID_ARGUMENT,
                        "unsupported kernel configuration (lanes per line 8: R 4,6,8; 16: R 1-4; 32: R 1,2,3,4,6,8)");
+    }
     if (c->lanes_per_line * 2 * c->regs_per_lane < h->nd)
         return h->fail(DS_INVALID_ARGUMENT, "kernel configuration holds fewer disparities than num_disparities");
     if (c->path_warps_per_block < 1 || c->path_warps_per_block > 8 || c->wta_threads < 32 || c->wta_threads > 256 ||
         c->wta_threads % 32 || (c->prefetch_steps != 4 && c->prefetch_steps != 8))
         return h->fail(DS_INVALID_ARGUMENT, "block shape or prefetch depth out of range");
-    if (c->fused_pairs) {
-        if (h->ndirs != 4) return h->fail(DS_INVALID_ARGUMENT, "fused pairs need 4 paths");
-        if (c->lanes_per_line == 8) return h->fail(DS_INVALID_ARGUMENT, "fused pairs need 16 or 32 lanes per line");
-        if (c->path_warps_per_block > 4 || c->horz_warps_per_block < 1 || c->horz_warps_per_block > 4)
-            return h->fail(DS_INVALID_ARGUMENT, "fused pairs: 1..4 warps per direction per block");
-        ds::KernelCfg t;
-        t.seg = c->lanes_per_line;
-        t.horz_warps = c->horz_warps_per_block;
-        if (horz_smem(h, t) > kMaxSmem) return h->fail(DS_INVALID_ARGUMENT, "fused pairs: rows per block exceed shared memory");
-    }
     return guarded(h, [&]() -> int {
         DS_CUDA(cudaStreamSynchronize(h->stream));
         h->cfg.R = c->regs_per_lane;
@@ -1631,6 +1654,7 @@ struct ds_batch {
     std::vector<dsk::PathArgs> a_paths;
     std::vector<dsk::WtaArgs> a_wta;
     std::vector<dsk::PostArgs> a_post;
+    std::vector<dsk::SweepArgs> a_sweep;  // by value into the graph: they name only the pair's own buffers
     dsk::RectifyArgs* d_rect = nullptr;
     dsk::CensusArgs* d_census = nullptr;
     dsk::CostArgs* d_costs = nullptr;
@@ -1641,8 +1665,10 @@ struct ds_batch {
         std::vector<int> pairs;  // heaviest first
         BatchGroup g_rect, g_post;
         std::vector<BatchGroup> g_census, g_costs, g_paths, g_wta;
+        std::vector<int> sweep;  // pairs on the sweep kernels: one column and one row launch each
         int launches() const {
-            return (g_rect.total > 0 ? 1 : 0) + static_cast<int>(g_census.size() + g_costs.size() + g_paths.size() + g_wta.size()) + 1;
+            return (g_rect.total > 0 ? 1 : 0) + static_cast<int>(g_census.size() + g_costs.size() + g_paths.size() + g_wta.size()) +
+                   2 * static_cast<int>(sweep.size()) + 1;
         }
     };
     std::vector<Micro> micro;  // pairs in micro-batches run through all stages back to back
@@ -1711,6 +1737,7 @@ void batch_fill_args(ds_batch* b) {
     b->a_paths.assign(n, {});
     b->a_wta.assign(n, {});
     b->a_post.assign(n, {});
+    b->a_sweep.assign(n, {});
     for (int i = 0; i < n; ++i) {
         ds_handle* h = b->h[i];
         const ds_pair_desc& d = b->desc[i];
@@ -1745,6 +1772,13 @@ void batch_fill_args(ds_batch* b) {
         ce.rx = sg.census_radius_x;
         ce.ry = sg.census_radius_y;
         ce.pitch = h->cpitch;
+        if (h->cfg.fused) {
+            // The sweep kernels read the left image as their guide from the pair's own buffer (an input of the
+            // caller can be re-bound without re-capturing the graph): raw pairs are rectified into it, the
+            // census kernel copies rectified inputs there.
+            if (!d.raw) ce.left_copy = h->d_rect[0];
+            b->a_sweep[i] = sweep_args(h);
+        }
         b->a_costs[i] = dsk::CostArgs{h->d_census[0], h->d_census[1], h->d_costs, h->w, h->h, h->nd, h->dp, sg.min_disparity,
                                       window, h->cpitch};
         auto& pa = b->a_paths[i];
@@ -1862,6 +1896,7 @@ void batch_bind_volumes(ds_batch* b) {
         for (int p : ps) {
             b->h[p]->d_values = mem;
             b->h[p]->d_costs = b->h[p]->costs_bytes ? static_cast<uint8_t*>(mem) + vb : nullptr;
+            bind_sweep_buffers(b->h[p]);
         }
     }
 }
@@ -1892,6 +1927,10 @@ void batch_plan_micro(ds_batch* b, ds_batch::Micro& m, const std::vector<int>& o
             add(g, i, tx * ty * 2, tx, ty);
         }
         const ds::KernelCfg& c = h->cfg;
+        if (c.fused) {
+            m.sweep.push_back(i);
+            continue;
+        }
         if (c.materialize) {
             BatchGroup& g = find_or_add(m.g_costs, [&](const BatchGroup& x) {
                 return x.cfg.R == c.R && x.cfg.seg == c.seg && x.c64 == h->census64;
@@ -1971,11 +2010,19 @@ void batch_enqueue_micro(ds_batch* b, const ds_batch::Micro& m, cudaStream_t st,
         ++g_launches;
     }
     mark(3);
+    for (int p : m.sweep) {
+        DS_CUDA(ds::launch_sweep_cols(b->h[p]->cfg, sweep_slant(b->h[p]), sweep_pad(b->h[p]), b->a_sweep[p], st));
+        ++g_launches;
+    }
     for (const auto& g : m.g_paths) {
         DS_CUDA(ds::launch_paths_batch(g.cfg, g.c64, g.wide, b->d_paths, g.dev(), st));
         ++g_launches;
     }
     mark(4);
+    for (int p : m.sweep) {
+        DS_CUDA(ds::launch_sweep_rows(b->h[p]->cfg, sweep_slant(b->h[p]), sweep_pad(b->h[p]), b->a_sweep[p], st));
+        ++g_launches;
+    }
     for (const auto& g : m.g_wta) {
         DS_CUDA(ds::launch_wta_batch(g.cfg, g.wide, g.ndirs, b->d_wta, g.dev(), g.smem, st));
         ++g_launches;
@@ -2054,16 +2101,8 @@ DS_API int ds_batch_create(const ds_pair_desc* pairs, int n, int n_calib, const 
         }
         b->h.push_back(h);
         if (d.kernel.regs_per_lane > 0) {
-            ds_kernel_config kc = d.kernel;
-            kc.fused_pairs = 0;  // the batched path runs the per-direction kernels
-            rc = ds_set_kernel_config(h, &kc);
+            rc = ds_set_kernel_config(h, &d.kernel);
             if (rc != DS_OK) g_error = "pair " + std::to_string(i) + ": " + h->err;
-        } else if (h->cfg.fused) {
-            h->cfg.fused = false;
-            rc = batch_guarded(b, [&] {
-                size_config_buffers(h);
-                return DS_OK;
-            });
         }
     }
     if (rc == DS_OK) {

@@ -13,7 +13,7 @@ namespace dsk {
 struct PathArgs;
 struct WtaArgs;
 struct CostArgs;
-struct FusedArgs;
+struct SweepArgs;
 }  // namespace dsk
 
 namespace ds {
@@ -26,8 +26,8 @@ struct KernelCfg {
     int paths_warps = 4;       // warps per block of the path kernel
     int prefetch = 4;          // steps of inputs in flight per scanline (4 or 8)
     int wta_threads = 256;     // threads per block of the WTA kernel
-    bool fused = true;         // 4 paths as two meet-in-the-middle pairs with the WTA fused (k_vert, k_horz_wta)
-    int horz_warps = 4;        // fused: warps per direction per block of k_horz_wta (rows = horz_warps * 32/SEG)
+    bool fused = true;         // 4 paths as the two sweep kernels (k_sweep_cols, k_sweep_rows with the WTA)
+    int horz_warps = 4;        // (kept in the configuration; the sweep kernels have fixed block shapes)
     int dp() const { return seg * 2 * R; }
 };
 
@@ -43,9 +43,10 @@ cudaError_t launch_paths(const KernelCfg& cfg, bool c64, bool wide, const dsk::P
                          cudaStream_t st);
 cudaError_t launch_wta(const KernelCfg& cfg, bool wide, const dsk::WtaArgs& a, int rows, size_t smem, cudaStream_t st);
 cudaError_t launch_costs(const KernelCfg& cfg, bool c64, const dsk::CostArgs& a, cudaStream_t st);
-// Fused pairs: `s16` = 16-bit vertical sums / horizontal scratch.
-cudaError_t launch_vert(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, cudaStream_t st);
-cudaError_t launch_horz(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, size_t smem, cudaStream_t st);
+// Sweep kernels (sweep_kernels.cuh): the vertical pair into S, then the horizontal pair with the WTA and the
+// L-R check. `pad`: nd < the slab disparities; `slant`: the k-2 / k+2 neighbours.
+cudaError_t launch_sweep_cols(const KernelCfg& cfg, bool slant, bool pad, const dsk::SweepArgs& a, cudaStream_t st);
+cudaError_t launch_sweep_rows(const KernelCfg& cfg, bool slant, bool pad, const dsk::SweepArgs& a, cudaStream_t st);
 
 struct BatchGroupDev;
 
@@ -61,8 +62,6 @@ cudaError_t launch_costs_batch(const KernelCfg& cfg, bool c64, const dsk::CostAr
     cudaError_t launch_paths_r##R(const KernelCfg&, bool, bool, const dsk::PathArgs&, int, int, cudaStream_t);      \
     cudaError_t launch_wta_r##R(const KernelCfg&, bool, const dsk::WtaArgs&, int, size_t, cudaStream_t);              \
     cudaError_t launch_costs_r##R(const KernelCfg&, bool, const dsk::CostArgs&, cudaStream_t);                      \
-    cudaError_t launch_vert_r##R(const KernelCfg&, bool, bool, const dsk::FusedArgs&, cudaStream_t);                \
-    cudaError_t launch_horz_r##R(const KernelCfg&, bool, bool, const dsk::FusedArgs&, size_t, cudaStream_t);        \
     cudaError_t launch_paths_batch_r##R(const KernelCfg&, bool, bool, const dsk::PathArgs*, const BatchGroupDev&,    \
                                         cudaStream_t);                                                               \
     cudaError_t launch_wta_batch_r##R(const KernelCfg&, bool, int, const dsk::WtaArgs*, const BatchGroupDev&, size_t,\

@@ -95,6 +95,7 @@ struct CensusArgs {
     const uint8_t* img[2];
     void* out[2];  // (y, x) at y * pitch + x
     int w, h, rx, ry, pitch;
+    uint8_t* left_copy;  // optional: the left image is also copied here (the sweep kernels' guide in batches)
 };
 
 // One 32 x 8 block of pixels per (bx, by): the block's image tile with its window halo is staged in
@@ -118,6 +119,7 @@ __device__ __forceinline__ void census_body(const CensusArgs& a, int bx, int by,
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
     if (x >= a.w || y >= a.h) return;
+    if (bz == 0 && a.left_copy) a.left_copy[static_cast<size_t>(y) * a.w + x] = tile[threadIdx.y + a.ry][threadIdx.x + a.rx];
     W word = 0;
     if (y >= a.ry && y < a.h - a.ry && x >= a.rx && x < a.w - a.rx) {
         const int cx = threadIdx.x + a.rx, cy = threadIdx.y + a.ry;

@@ -3,7 +3,6 @@
 
 #include "batch_common.cuh"
 #include "dispatch.h"
-#include "fused_kernels.cuh"
 #include "stereo_kernels.cuh"
 
 namespace ds {
@@ -51,43 +50,6 @@ cudaError_t costs_t(const dsk::CostArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <int R, int SEG, typename CW, typename SV>
-cudaError_t vert_t(const KernelCfg& cfg, const dsk::FusedArgs& a, cudaStream_t st) {
-    const int nwd = cfg.paths_warps;
-    const int cols = nwd * (32 / SEG);
-    const dim3 grid((a.w + cols - 1) / cols);
-    if (cfg.prefetch == 8) dsk::k_vert<R, SEG, CW, SV, 8><<<grid, 64 * nwd, 0, st>>>(a);
-    else dsk::k_vert<R, SEG, CW, SV, 4><<<grid, 64 * nwd, 0, st>>>(a);
-    return cudaGetLastError();
-}
-
-template <int R, int SEG, typename CW, typename SV>
-cudaError_t horz_t(const KernelCfg& cfg, const dsk::FusedArgs& a, size_t smem, cudaStream_t st) {
-    const int nrw = cfg.horz_warps;
-    const int rows = nrw * (32 / SEG);
-    const dim3 grid((a.h + rows - 1) / rows);
-    auto k = cfg.prefetch == 8 ? dsk::k_horz_wta<R, SEG, CW, SV, 8> : dsk::k_horz_wta<R, SEG, CW, SV, 4>;
-    if (smem > 48 * 1024) {
-        const cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        if (e != cudaSuccess) return e;
-    }
-    k<<<grid, 64 * nrw, smem, st>>>(a);
-    return cudaGetLastError();
-}
-
-template <int R, int SEG>
-cudaError_t vert_seg(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, cudaStream_t st) {
-    if (c64) return s16 ? vert_t<R, SEG, uint64_t, uint16_t>(cfg, a, st) : vert_t<R, SEG, uint64_t, uint8_t>(cfg, a, st);
-    return s16 ? vert_t<R, SEG, uint32_t, uint16_t>(cfg, a, st) : vert_t<R, SEG, uint32_t, uint8_t>(cfg, a, st);
-}
-
-template <int R, int SEG>
-cudaError_t horz_seg(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, size_t smem, cudaStream_t st) {
-    if (c64)
-        return s16 ? horz_t<R, SEG, uint64_t, uint16_t>(cfg, a, smem, st) : horz_t<R, SEG, uint64_t, uint8_t>(cfg, a, smem, st);
-    return s16 ? horz_t<R, SEG, uint32_t, uint16_t>(cfg, a, smem, st) : horz_t<R, SEG, uint32_t, uint8_t>(cfg, a, smem, st);
-}
-
 }  // namespace ds
 
 // SEG 16 exists for R <= 4 only.
@@ -121,14 +83,6 @@ cudaError_t horz_seg(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedA
         DS_SEG_SWITCH(R,                                                                                             \
                       (c64 ? costs_t<R, (R <= 4 ? 16 : 32), uint64_t>(a, st) : costs_t<R, (R <= 4 ? 16 : 32), uint32_t>(a, st)), \
                       (c64 ? costs_t<R, 32, uint64_t>(a, st) : costs_t<R, 32, uint32_t>(a, st)))                     \
-    }                                                                                                                \
-    cudaError_t launch_vert_r##R(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, cudaStream_t st) { \
-        DS_SEG_SWITCH(R, (vert_seg<R, (R <= 4 ? 16 : 32)>(cfg, c64, s16, a, st)), (vert_seg<R, 32>(cfg, c64, s16, a, st))) \
-    }                                                                                                                \
-    cudaError_t launch_horz_r##R(const KernelCfg& cfg, bool c64, bool s16, const dsk::FusedArgs& a, size_t smem,     \
-                                 cudaStream_t st) {                                                                  \
-        DS_SEG_SWITCH(R, (horz_seg<R, (R <= 4 ? 16 : 32)>(cfg, c64, s16, a, smem, st)),                              \
-                      (horz_seg<R, 32>(cfg, c64, s16, a, smem, st)))                                                 \
     }                                                                                                                \
     }
 

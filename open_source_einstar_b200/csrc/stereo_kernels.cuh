@@ -25,6 +25,9 @@ namespace dsk {
 constexpr float kInvalid = -1.0e9f;  // depth::kInvalidDisparity (stereo.hpp:23)
 constexpr int kNoMatch = INT_MIN;    // sgm_disparity's kNoMatch (stereo.cpp:413)
 constexpr int kMaxDisparities = 512;
+// Guard rows above and below the census, guide and sweep buffers (>= the deepest prefetch ring), so that
+// prefetches past a scanline's end stay inside the allocation.
+constexpr int kGuardRows = 8;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 __host__ __device__ inline bool valid_disparity(float d) { return d > -1.0e8f; }  // stereo.hpp:24
@@ -251,11 +254,12 @@ template <int SEG>
 __device__ __forceinline__ uint32_t seg_min(uint32_t v, int seg) {
     if constexpr (SEG == 32) {
         return __reduce_min_sync(kFull, v);
-    } else if constexpr (SEG == 8) {  // four segments per warp: one butterfly serves all of them
-        v = min(v, __shfl_xor_sync(kFull, v, 4));
-        v = min(v, __shfl_xor_sync(kFull, v, 2));
-        return min(v, __shfl_xor_sync(kFull, v, 1));
+    } else if constexpr (SEG <= 8) {  // 4 or 8 segments per warp: one butterfly serves all of them
+#pragma unroll
+        for (int off = SEG / 2; off >= 1; off /= 2) v = min(v, __shfl_xor_sync(kFull, v, off));
+        return v;
     } else {
+        static_assert(SEG == 16, "segments of 4, 8, 16 or 32 lanes");
         const uint32_t r0 = __reduce_min_sync(kFull, seg == 0 ? v : 0xFFFFFFFFu);
         const uint32_t r1 = __reduce_min_sync(kFull, seg == 1 ? v : 0xFFFFFFFFu);
         return seg == 0 ? r0 : r1;

@@ -4,8 +4,8 @@ import json
 import numpy as np
 import pytest
 
-from open_source_einstar_b200.autotune import (SUPPORTED, Autotuner, FrameKind, batch_schedules, search,
-                                               stage_candidates, tile_shapes)
+from open_source_einstar_b200.autotune import (SUPPORTED, SWEEP_SHAPES, Autotuner, FrameKind, batch_schedules, search,
+                                               stage_candidates, sweep_shapes, tile_shapes)
 
 
 @pytest.mark.parametrize("d", [4, 16, 24, 32, 40, 64, 96, 128, 192, 256, 384, 512])
@@ -38,9 +38,33 @@ def test_staged_search_finds_the_fastest_of_each_stage():
     assert n <= 30  # staged: two shapes go through the block search, not the full product (~100)
 
 
+@pytest.mark.parametrize("d", [4, 24, 40, 48, 64, 96, 128])
+def test_sweep_shapes_cover_the_disparities_with_least_padding(d):
+    shapes = sweep_shapes(d)
+    assert shapes
+    for r, seg in shapes:
+        assert r in SWEEP_SHAPES[seg] and seg * 2 * r >= d
+        assert all(seg * 2 * x < d for x in SWEEP_SHAPES[seg] if x < r)
+
+
+def test_sweep_candidates_only_where_the_kernels_fit():
+    from open_source_einstar_b200 import SgmParams, StereoParams
+    fits = FrameKind.of(1280, 1024, StereoParams(sgm=SgmParams(num_disparities=128)))
+    assert fits.sweep_fit()
+    sweeps = [c for c in stage_candidates(fits, 1) if c.get("fused_pairs")]
+    assert [(c["regs_per_lane"], c["lanes_per_line"]) for c in sweeps] == [(8, 8)]
+    assert not [c for c in stage_candidates(fits, 1, fused_ok=False) if c.get("fused_pairs")]
+    for sp in (SgmParams(num_disparities=128, eight_paths=True),          # 8 paths
+               SgmParams(num_disparities=192),                            # D > 128
+               SgmParams(num_disparities=64, p2=120),                     # 2 (window + P2) > 255
+               SgmParams(num_disparities=64, census_radius_x=3, census_radius_y=3)):  # 48 neighbours
+        kind = FrameKind.of(640, 512, StereoParams(sgm=sp))
+        assert not kind.sweep_fit() and not [c for c in stage_candidates(kind, 1) if c.get("fused_pairs")]
+
+
 def test_rejected_configurations_are_skipped():
     kind = FrameKind(640, 512, 64, eight_paths=True)
-    assert all(not c.get("fused_pairs") for c in stage_candidates(kind, 1))  # fused pairs need 4 paths
+    assert all(not c.get("fused_pairs") for c in stage_candidates(kind, 1))  # the sweep kernels need 4 paths
     best, _ = search(kind, lambda c: float("inf") if c["lanes_per_line"] != 32 else 1.0)
     assert best["lanes_per_line"] == 32
 
@@ -61,7 +85,7 @@ def test_table_roundtrip(tmp_path):
 def test_frame_kind_from_params():
     from open_source_einstar_b200 import SgmParams, StereoParams
     k = FrameKind.of(1280, 1024, StereoParams(sgm=SgmParams(num_disparities=256, eight_paths=True, p2=300)))
-    assert k == FrameKind(1280, 1024, 256, True, True, 25)
+    assert k == FrameKind(1280, 1024, 256, True, True, 25, False)
 
 
 def test_batch_schedules():

@@ -215,23 +215,32 @@ def test_errors_follow_the_reference(cuda, golden):
 
 
 SUPPORTED = [(r, 8) for r in (4, 6, 8)] + [(r, 16) for r in (1, 2, 3, 4)] + [(r, 32) for r in (1, 2, 3, 4, 6, 8)]
+SWEEP = [(6, 4), (8, 4), (6, 8), (8, 8)]  # (regs per lane, lanes per line) of the sweep kernels
+
+
+def _sweep_fit(p: OracleSgm, w, h):
+    from open_source_einstar_b200 import SgmParams, StereoParams
+    from open_source_einstar_b200.autotune import FrameKind
+    return FrameKind.of(w, h, StereoParams(sgm=SgmParams(**p.__dict__))).sweep_fit()
 
 
 @pytest.mark.parametrize("mode", ["per_direction", "materialized", "fused_pairs"])
 def test_every_kernel_config_is_bit_exact(cuda, golden, port, mode):
-    """All (lanes per line, regs per lane) configurations and all SGM kernel modes give identical bytes."""
+    """All (lanes per line, regs per lane) configurations and all SGM kernel modes give identical bytes;
+    fused_pairs runs the sweep kernels in each of their shapes."""
     for name in ("plane_sphere_160x128", "d_not_multiple_of_32_d40", "eight_paths", "census_9x7_wide", "tiny_37x29_d5",
-                 "census_7x7_u64", "negative_min_disparity", "no_subpixel_uniq08_lr2"):
+                 "census_7x7_u64", "negative_min_disparity", "no_subpixel_uniq08_lr2", "no_slant_fixed_p2",
+                 "unmatched_noise"):
         c = golden[name]
         p = OracleSgm(**c["params"])
-        if mode == "fused_pairs" and p.eight_paths:
-            continue
         h, w = c["shape"]
+        if mode == "fused_pairs" and not _sweep_fit(p, w, h):
+            continue
         want = c["median"]
-        for r, seg in SUPPORTED:
-            if 2 * r * seg < p.num_disparities or (seg == 8 and mode == "fused_pairs"):
+        for r, seg in (SWEEP if mode == "fused_pairs" else SUPPORTED):
+            if 2 * r * seg < p.num_disparities:
                 continue
-            for pf in (4, 8):
+            for pf in ((4,) if mode == "fused_pairs" else (4, 8)):
                 with _stereo(p, w, h, c["subpixel"], median=True) as s:
                     s.set_kernel_config(r, seg, mode == "materialized", path_warps_per_block=2 if r > 4 else 4,
                                         wta_threads=128, prefetch_steps=pf, fused_pairs=mode == "fused_pairs",
@@ -249,10 +258,12 @@ def test_odd_and_degenerate_sizes(cuda, port, w, h, nd, mind):
     right = base[:, 14:14 + w].copy()
     p = OracleSgm(min_disparity=mind, num_disparities=nd)
     want = port.median3(port.sgm_disparity(left, right, p))
+    from open_source_einstar_b200.autotune import sweep_shapes
     for fused in (False, True):
         with _stereo(p, w, h, median=True) as s:
             cfg = s.kernel_config()
-            s.set_kernel_config(cfg["regs_per_lane"], cfg["lanes_per_line"], False, 1, 64, 4, fused, 1)
+            r, seg = sweep_shapes(nd)[0] if fused else (cfg["regs_per_lane"], cfg["lanes_per_line"])
+            s.set_kernel_config(r, seg, False, 1, 64, 4, fused, 1)
             got = s.compute(left, right).disparity
         assert same_bits(got, want), f"{w}x{h} fused={fused}: {mismatch_report(got, want)}"
 
@@ -263,23 +274,28 @@ def test_batch_matches_per_pair_runs(cuda, port):
     import torch
     from open_source_einstar_b200 import (CudaStereo, PairDesc, RectifiedGeometry, RemapTable, SgmParams, StereoBatch,
                                           StereoParams, synth)
+    sweep = {"fused_pairs": 1, "materialize_costs": 0}
     specs = [(320, 256, 64, None), (160, 128, 96, None), (240, 192, 128, None), (200, 136, 192, None),
              (160, 128, 40, {"regs_per_lane": 3, "lanes_per_line": 16, "materialize_costs": 0}),
-             (128, 96, 64, {"regs_per_lane": 1, "lanes_per_line": 32, "materialize_costs": 1, "prefetch_steps": 8})]
+             (128, 96, 64, {"regs_per_lane": 1, "lanes_per_line": 32, "materialize_costs": 1, "prefetch_steps": 8}),
+             (240, 192, 128, {"regs_per_lane": 8, "lanes_per_line": 8, **sweep}),
+             (160, 128, 40, {"regs_per_lane": 6, "lanes_per_line": 4, **sweep}),
+             (200, 136, 96, {"regs_per_lane": 6, "lanes_per_line": 8, **sweep})]
     rect_pairs = [synth.plane_sphere_pair(seed=40 + i, width=w, height=h, f=w * 1.4, num_disparities=d)
                   for i, (w, h, d, _) in enumerate(specs)]
-    raw_specs = [(256, 192, 0), (256, 192, 0), (192, 160, 1)]
+    raw_specs = [(256, 192, 0, None), (256, 192, 0, {"regs_per_lane": 8, "lanes_per_line": 4, **sweep}), (192, 160, 1, None)]
     raw_pairs = [synth.raw_objects_pair(seed=60 + i, width=w, height=h, f=w * 0.86, num_disparities=64, n_objects=6,
-                                        device="cuda") for i, (w, h, _) in enumerate(raw_specs)]
+                                        device="cuda") for i, (w, h, _, _) in enumerate(raw_specs)]
     descs, inputs, want = [], [], []
     for (w, h, d, k), pr in zip(specs, rect_pairs):
         sp = StereoParams(sgm=SgmParams(min_disparity=pr.min_disparity, num_disparities=d))
         descs.append(PairDesc(w, h, sp, geometry=RectifiedGeometry(pr.f, 0, 0, pr.baseline), kernel=k))
         inputs.append((pr.left, pr.right))
     calibs = {}
-    for (w, h, ci), pr in zip(raw_specs, raw_pairs):
+    first_raw = len(descs)
+    for (w, h, ci, k), pr in zip(raw_specs, raw_pairs):
         sp = StereoParams(sgm=SgmParams(min_disparity=pr.min_disparity, num_disparities=64))
-        descs.append(PairDesc(w, h, sp, raw=True, calib=ci))
+        descs.append(PairDesc(w, h, sp, raw=True, calib=ci, kernel=k))
         inputs.append((pr.left, pr.right))
         calibs.setdefault(ci, (pr.maps, w, h))
     for d, (l, r), i in zip(descs, inputs, range(len(descs))):
@@ -287,7 +303,8 @@ def test_batch_matches_per_pair_runs(cuda, port):
             if d.kernel:
                 kk = {"path_warps_per_block": 4, "wta_threads": 256, "prefetch_steps": 4, **d.kernel}
                 s.set_kernel_config(kk["regs_per_lane"], kk["lanes_per_line"], bool(kk.get("materialize_costs", 0)),
-                                    kk["path_warps_per_block"], kk["wta_threads"], kk["prefetch_steps"])
+                                    kk["path_warps_per_block"], kk["wta_threads"], kk["prefetch_steps"],
+                                    bool(kk.get("fused_pairs", 0)))
             if d.raw:
                 (mlx, mly), (mrx, mry) = calibs[d.calib][0]
                 s.set_rectification(RemapTable(mlx, mly), RemapTable(mrx, mry), d.width, d.height)
@@ -325,11 +342,21 @@ def test_batch_matches_per_pair_runs(cuda, port):
                 assert np.array_equal(o["disparity_u16"].cpu().numpy().view(np.uint16), wres.disparity_u16)
                 if "depth" in o:
                     assert same_bits(o["depth"].cpu().numpy(), wres.depth)
-        # re-bind: pair 6 takes pair 7's inputs (same size and calibration); the captured graph is replayed
-        b.bind(6, dev_in[7][0], dev_in[7][1], dev_out[6])
+        # re-bind: the first raw pair takes the second's inputs (same size and calibration; the second runs on
+        # the sweep kernels); the captured graph is replayed
+        b.bind(first_raw, dev_in[first_raw + 1][0], dev_in[first_raw + 1][1], dev_out[first_raw])
         b.run(stream=st)
         st.synchronize()
-        assert same_bits(dev_out[6]["disparity"].cpu().numpy(), want[7].disparity)
+        assert same_bits(dev_out[first_raw]["disparity"].cpu().numpy(), want[first_raw + 1].disparity)
+        # re-bind a rectified sweep pair to new buffers with its inputs and scribble over the old ones: the
+        # sweep kernels' guide (the census kernel's copy of the left image) follows the binding
+        nl, nr = dev_in[6][0].clone(), dev_in[6][1].clone()
+        b.bind(6, nl, nr, dev_out[6])
+        dev_in[6][0].fill_(77)
+        dev_in[6][1].fill_(13)
+        b.run(stream=st)
+        st.synchronize()
+        assert same_bits(dev_out[6]["disparity"].cpu().numpy(), want[6].disparity)
         if branches == 1:  # one persistent launch per stage and kernel variant for all pairs
             assert b.launches_per_run < 5 * len(descs) // 2
         b.close()
