@@ -194,7 +194,7 @@ DS_API uint64_t ds_kernel_launches(void);
  * regs 1..4; 32 lanes with regs 1, 2, 3, 4, 6, 8. materialize_costs: write the matching-cost volume once
  * instead of recomputing costs from the census in every direction. fused_pairs selects the sweep kernels
  * instead: the vertical path pair, then the horizontal pair with the WTA and the L-R check (two launches
- * per frame, 6 bytes of volume traffic per pixel and disparity). They need 4 paths, census windows of at
+ * per frame, 8 bytes of volume traffic per pixel and disparity). They need 4 paths, census windows of at
  * most 32 neighbours, 2 (window + P2) <= 255, and 4 or 8 lanes per line with regs 6 or 8 (D <= 128).
  * Results are identical for every configuration; only speed differs (the autotuner chooses). */
 typedef struct ds_kernel_config {

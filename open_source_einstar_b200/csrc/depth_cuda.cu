@@ -84,10 +84,12 @@ struct ds_handle {
     void* census_raw[2] = {nullptr, nullptr};
     int cpitch = 0, cguard = 0;
     size_t census_bytes = 0;                   // per image, guards included (capacity)
-    // Sweep kernels (cfg.fused), all inside d_values: vertical pair sums S and horizontal first-half values T
-    // (u8 slabs with guard rows), the row kernel's per-pixel WTA records and its right-WTA keys.
+    // Sweep kernels (cfg.fused), all inside d_values: vertical pair sums S, horizontal first-half values T and
+    // the column kernel's costs C (u8 slabs with guard rows), the row kernel's per-pixel WTA records and its
+    // right-WTA keys.
     void* d_S = nullptr;
     void* d_T = nullptr;
+    void* d_C = nullptr;
     uint2* d_rec = nullptr;
     uint16_t* d_rk = nullptr;
     void* d_values = nullptr;
@@ -276,6 +278,7 @@ dsk::SweepArgs sweep_args(const ds_handle* h) {
     a.guide = h->d_rect[0];
     a.S = static_cast<uint8_t*>(h->d_S);
     a.T = static_cast<uint8_t*>(h->d_T);
+    a.C = static_cast<uint8_t*>(h->d_C);
     a.rec = h->d_rec;
     a.rk = h->d_rk;
     a.disp = h->d_disp_lr;
@@ -387,18 +390,18 @@ void free_counted(ds_handle* h, void*& p, size_t bytes) {
     }
 }
 
-// The sweep kernels' buffers inside the path-value volume: S and T slabs (u8 [y][x][dp] with kGuardRows guard
-// rows above and below), then the WTA records (8 bytes per pixel) and the right-WTA keys (2 x 2 bytes).
+// The sweep kernels' buffers inside the path-value volume: S, T and C slabs (u8 [y][x][dp] with kGuardRows
+// guard rows above and below), then the WTA records (8 bytes per pixel) and the right-WTA keys (2 x 2 bytes).
 size_t sweep_slab_bytes(const ds_handle* h) {
     return (static_cast<size_t>(h->h + 2 * dsk::kGuardRows) * h->w * h->dp + 255) / 256 * 256;
 }
 size_t sweep_volume_bytes(const ds_handle* h) {
     const size_t n = static_cast<size_t>(h->w) * h->h;
-    return 2 * sweep_slab_bytes(h) + (n * 8 + 255) / 256 * 256 + n * 4;
+    return 3 * sweep_slab_bytes(h) + (n * 8 + 255) / 256 * 256 + n * 4;
 }
 void bind_sweep_buffers(ds_handle* h) {
     if (!h->cfg.fused || !h->d_values) {
-        h->d_S = h->d_T = nullptr;
+        h->d_S = h->d_T = h->d_C = nullptr;
         h->d_rec = nullptr;
         h->d_rk = nullptr;
         return;
@@ -408,8 +411,9 @@ void bind_sweep_buffers(ds_handle* h) {
     uint8_t* base = static_cast<uint8_t*>(h->d_values);
     h->d_S = base + lead;
     h->d_T = base + slab + lead;
-    h->d_rec = reinterpret_cast<uint2*>(base + 2 * slab);
-    h->d_rk = reinterpret_cast<uint16_t*>(base + 2 * slab + (n * 8 + 255) / 256 * 256);
+    h->d_C = base + 2 * slab + lead;
+    h->d_rec = reinterpret_cast<uint2*>(base + 3 * slab);
+    h->d_rk = reinterpret_cast<uint16_t*>(base + 3 * slab + (n * 8 + 255) / 256 * 256);
 }
 
 constexpr int kCensusSlack = 40;

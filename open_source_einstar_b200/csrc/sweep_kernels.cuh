@@ -11,9 +11,12 @@
 //                 diagonals (:434-447). An epilogue over the block's rows finishes the float part (uniqueness,
 //                 parabola) and the L-R check (:450-461).
 //
-// Costs are recomputed from the census words in every direction (popcount runs on its own pipe), so the
-// only per-disparity traffic is S (written twice, read twice) and T (written and read once): 6 bytes per
-// pixel and disparity instead of the cost volume plus four direction slabs.
+// Costs are computed from the census words: once per pixel in the column kernel (each direction computes the
+// rows of its first half and stores them as bytes in C; its second half reads the other direction's), and
+// again in each direction of the row kernel, where the right census words come through a sliding window
+// in registers (popcount runs on its own pipe). Per-disparity traffic: S written twice and read twice, C
+// written and read once, T written and read once: 8 bytes per pixel and disparity, instead of the cost
+// volume plus four direction slabs.
 //
 // Lane layout. SEG lanes run one scanline; lane sl holds NV = 2R disparities k0 = sl*NV .. k0+NV-1 in R
 // registers of two 16-bit lanes, register r holding slots (r, r + R). The k-1 / k+1 / k-2 / k+2 neighbours of
@@ -47,6 +50,7 @@ struct SweepArgs {
     const uint8_t* guide;      // left rectified image, (y, x) at y * w + x; guard rows readable
     uint8_t* S;                // [y][x][dp] vertical pair sums (guard rows)
     uint8_t* T;                // [y][x][dp] first-half values of the horizontal sweeps (guard rows)
+    uint8_t* C;                // [y][x][dp] matching costs of the column kernel's first halves (guard rows)
     uint2* rec;                // [y][x] left WTA of the row kernel: (key | second << 16, cost(k-1) | cost(k+1) << 16)
     uint16_t* rk;              // [2][y][x] right-WTA keys of the left-to-right and right-to-left sweeps
     float* disp;               // L-R checked disparity [y][x]
@@ -70,6 +74,16 @@ __device__ __forceinline__ void sw_block_barrier() { asm volatile("barrier.sync 
 template <int SEG>
 __device__ __forceinline__ uint32_t sw_seg_min2(uint32_t lmin2, int seg) {
     return seg_min<SEG>(vmin2(lmin2, prmt(lmin2, lmin2, 0x1032)), seg);
+}
+
+// Minimum of v[0..N) into v[0] by a tree (a short dependency chain); v is overwritten.
+template <int N>
+__device__ __forceinline__ uint32_t sw_tree_min(uint32_t (&v)[N]) {
+#pragma unroll
+    for (int n = N; n > 1; n = (n + 1) / 2)
+#pragma unroll
+        for (int r = 0; r < n / 2; ++r) v[r] = vmin2(v[r], v[r + (n + 1) / 2]);
+    return v[0];
 }
 
 template <int R>
@@ -125,12 +139,9 @@ __device__ __forceinline__ void sw_step(uint32_t (&v)[R], uint32_t& pm2, const u
         if constexpr (PAD) L = (L & ~pad[r]) | (INF2 & pad[r]);
         out[r] = L;
     }
-    uint32_t lmin = out[0];
-#pragma unroll
-    for (int r = 1; r < R; ++r) lmin = vmin2(lmin, out[r]);
-    pm2 = sw_seg_min2<SEG>(lmin, seg);
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = out[r];
+    pm2 = sw_seg_min2<SEG>(sw_tree_min<R>(out), seg);
 }
 
 // The first pixel of a scanline: L = C (padding slots INF).
@@ -170,6 +181,8 @@ __device__ __forceinline__ void sw_costs_aligned(uint32_t lw, const uint32_t (&q
 // base + wi + 4 * seg (one per segment), so that all its columns have the same residue mod 4: the right
 // census words of every lane then start at the same offset within a 16-byte line, and each lane loads its
 // NV words with NQ aligned 128-bit loads. A block covers 4 * (32 / SEG) columns.
+// First half of a column: costs from the census (stored to C), path values to S. Second half: costs from
+// C (the other direction's first half), S += own path values.
 
 template <int R, int SEG, bool SLANT, bool PAD, int PF>
 __device__ __forceinline__ void sweep_cols_body(const SweepArgs& a, const uint32_t* __restrict__ p2t, int bx) {
@@ -207,93 +220,110 @@ __device__ __forceinline__ void sweep_cols_body(const SweepArgs& a, const uint32
     const int n1 = down ? mid : a.h - mid, n2 = a.h - n1;
     const long cst = static_cast<long>(dy) * a.cpitch, gst = static_cast<long>(dy) * a.w;
     const long sst = static_cast<long>(dy) * a.w * a.dp;
-
-    const uint32_t *fl, *fq;
-    const uint8_t *fg, *fs;
-    auto seek = [&](int s) {
-        const long y = y0 + static_cast<long>(s) * dy;
-        fl = a.census_l + y * a.cpitch + xs;
-        fq = a.census_r + y * a.cpitch + qb;
-        fg = a.guide + y * a.w + xs;
-        fs = a.S + (y * a.w + xs) * a.dp + k0;
-    };
-    int rI[PF];
-    uint32_t rl[PF], rq[PF][NW], rs[PF][CW];
-    auto fetch = [&](int u, bool with_s) {
-        rI[u] = __ldg(fg);
-        rl[u] = __ldg(fl);
-#pragma unroll
-        for (int i = 0; i < NQ; ++i) {
-            const uint4 t = __ldg(reinterpret_cast<const uint4*>(fq) + i);
-            rq[u][4 * i] = t.x, rq[u][4 * i + 1] = t.y, rq[u][4 * i + 2] = t.z, rq[u][4 * i + 3] = t.w;
-        }
-        if (with_s) ld_chunk<NV, LD_CG>(fs, rs[u]);
-        fl += cst;
-        fq += cst;
-        fg += gst;
-        fs += sst;
-    };
-    auto costs = [&](int u, uint32_t (&c)[R]) {
-        switch (al) {
-            case 0: sw_costs_aligned<R, 0, NW>(rl[u], rq[u], c); break;
-            case 1: sw_costs_aligned<R, 1, NW>(rl[u], rq[u], c); break;
-            case 2: sw_costs_aligned<R, 2, NW>(rl[u], rq[u], c); break;
-            default: sw_costs_aligned<R, 3, NW>(rl[u], rq[u], c); break;
-        }
-        if (border) {
-#pragma unroll
-            for (int r = 0; r < R; ++r) c[r] = (c[r] & vm[r]) | (inv2 & ~vm[r]);
-        }
-    };
+    const long pix0 = (static_cast<long>(y0) * a.w + xs) * a.dp + k0;  // S / C offset at the first row
 
     uint32_t v[R], pm2 = 0, c[R], w[CW];
     int last = 0;
-    uint8_t* ps = a.S + (static_cast<long>(y0) * a.w + xs) * a.dp + k0;
-    seek(0);
+    // ---- first half: costs from the census words
+    {
+        const uint32_t* fl = a.census_l + static_cast<long>(y0) * a.cpitch + xs;
+        const uint32_t* fq = a.census_r + static_cast<long>(y0) * a.cpitch + qb;
+        const uint8_t* fg = a.guide + static_cast<long>(y0) * a.w + xs;
+        int rI[PF];
+        uint32_t rl[PF], rq[PF][NW];
+        auto fetch = [&](int u) {
+            rI[u] = __ldg(fg);
+            rl[u] = __ldg(fl);
 #pragma unroll
-    for (int u = 0; u < PF; ++u)
-        if (u < n1) fetch(u, false);
-    for (int base = 0; base < n1; base += PF) {
-#pragma unroll
-        for (int u = 0; u < PF; ++u) {
-            const int s = base + u;
-            if (s >= n1) break;
-            costs(u, c);
-            const uint32_t p2v = sw_p2(p2t, rI[u], last);
-            if (s + PF < n1) fetch(u, false);
-            if (s == 0) sw_first<R, SEG, PAD>(v, pm2, c, INF2, pad, seg);
-            else sw_step<R, SEG, SLANT, PAD>(v, pm2, c, pm2 + p2v, INF2, P12, pad, sl, seg);
-            if (live) {
-                sw_pack<R>(v, w);
-                st_chunk<NV, false>(ps, w);
+            for (int i = 0; i < NQ; ++i) {
+                const uint4 t = __ldg(reinterpret_cast<const uint4*>(fq) + i);
+                rq[u][4 * i] = t.x, rq[u][4 * i + 1] = t.y, rq[u][4 * i + 2] = t.z, rq[u][4 * i + 3] = t.w;
             }
-            ps += sst;
+            fl += cst;
+            fq += cst;
+            fg += gst;
+        };
+        uint8_t* ps = a.S + pix0;
+        uint8_t* pc = a.C + pix0;
+#pragma unroll
+        for (int u = 0; u < PF; ++u)
+            if (u < n1) fetch(u);
+        for (int base = 0; base < n1; base += PF) {
+#pragma unroll
+            for (int u = 0; u < PF; ++u) {
+                const int s = base + u;
+                if (s >= n1) break;
+                switch (al) {
+                    case 0: sw_costs_aligned<R, 0, NW>(rl[u], rq[u], c); break;
+                    case 1: sw_costs_aligned<R, 1, NW>(rl[u], rq[u], c); break;
+                    case 2: sw_costs_aligned<R, 2, NW>(rl[u], rq[u], c); break;
+                    default: sw_costs_aligned<R, 3, NW>(rl[u], rq[u], c); break;
+                }
+                if (border) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) c[r] = (c[r] & vm[r]) | (inv2 & ~vm[r]);
+                }
+                const uint32_t p2v = sw_p2(p2t, rI[u], last);
+                if (s + PF < n1) fetch(u);
+                if (live) {
+                    sw_pack<R>(c, w);
+                    st_chunk<NV, false>(pc, w);
+                }
+                if (s == 0) sw_first<R, SEG, PAD>(v, pm2, c, INF2, pad, seg);
+                else sw_step<R, SEG, SLANT, PAD>(v, pm2, c, pm2 + p2v, INF2, P12, pad, sl, seg);
+                if (live) {
+                    sw_pack<R>(v, w);
+                    st_chunk<NV, false>(ps, w);
+                }
+                ps += sst;
+                pc += sst;
+            }
         }
     }
-    __syncthreads();  // the other direction's first-half values are in S
-    seek(n1);
+    __syncthreads();  // the other direction's first-half values and costs are in S and C
+    // ---- second half: costs from C, S += own values
+    {
+        const long off = static_cast<long>(n1) * dy;
+        const uint8_t* fg = a.guide + (static_cast<long>(y0) + off) * a.w + xs;
+        const uint8_t* fc = a.C + pix0 + off * a.w * a.dp;
+        uint8_t* ps = a.S + pix0 + off * a.w * a.dp;
+        int rI[PF];
+        uint32_t rc[PF][CW], rs[PF][CW];
+        auto fetch = [&](int u, int i) {  // ring slot u <- step (current + i)
+            rI[u] = __ldg(fg + i * gst);
+            ld_chunk<NV, LD_CG>(fc + i * sst, rc[u]);
+            ld_chunk<NV, LD_CG>(ps + i * sst, rs[u]);
+        };
 #pragma unroll
-    for (int u = 0; u < PF; ++u)
-        if (u < n2) fetch(u, true);
-    for (int base = 0; base < n2; base += PF) {
+        for (int u = 0; u < PF; ++u)
+            if (u < n2) fetch(u, u);
+        for (int base = 0; base < n2; base += PF) {
 #pragma unroll
-        for (int u = 0; u < PF; ++u) {
-            const int s = base + u;
-            if (s >= n2) break;
-            costs(u, c);
-            const uint32_t p2v = sw_p2(p2t, rI[u], last);
-            uint32_t o[R];
-            sw_unpack<R>(rs[u], o);
-            if (s + PF < n2) fetch(u, true);
-            if (n1 == 0 && s == 0) sw_first<R, SEG, PAD>(v, pm2, c, INF2, pad, seg);
-            else sw_step<R, SEG, SLANT, PAD>(v, pm2, c, pm2 + p2v, INF2, P12, pad, sl, seg);
+            for (int u = 0; u < PF; ++u) {
+                const int s = base + u;
+                if (s >= n2) break;
+                uint32_t o[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) o[r] += PAD ? (v[r] & ~pad[r]) : v[r];
-            if (live) {
-                sw_pack<R>(o, w);
-                st_chunk<NV, false>(ps, w);
+                for (int i = 0; i < CW; ++i) {
+                    c[2 * i] = prmt(rc[u][i], 0u, 0x4240);
+                    c[2 * i + 1] = prmt(rc[u][i], 0u, 0x4341);
+                    o[2 * i] = prmt(rs[u][i], 0u, 0x4240);
+                    o[2 * i + 1] = prmt(rs[u][i], 0u, 0x4341);
+                }
+                const uint32_t p2v = sw_p2(p2t, rI[u], last);
+                if (s + PF < n2) fetch(u, PF);
+                if (n1 == 0 && s == 0) sw_first<R, SEG, PAD>(v, pm2, c, INF2, pad, seg);
+                else sw_step<R, SEG, SLANT, PAD>(v, pm2, c, pm2 + p2v, INF2, P12, pad, sl, seg);
+#pragma unroll
+                for (int r = 0; r < R; ++r) o[r] += PAD ? (v[r] & ~pad[r]) : v[r];
+                if (live) {
+                    sw_pack<R>(o, w);
+                    st_chunk<NV, false>(ps, w);
+                }
+                ps += sst;
+                fc += sst;
+                fg += gst;
             }
-            ps += sst;
         }
     }
 }
@@ -307,28 +337,32 @@ __device__ __forceinline__ void sweep_cols_body(const SweepArgs& a, const uint32
 // lane is the one leaving its neighbour (one shuffle), and only the lane at the end of the segment loads
 // a new word (the same address for the whole segment).
 //
-// Right WTA: candidate (x, k) belongs to right pixel xr = x - min - k. Each lane keeps, per slot j, the
-// running minimum key of the right pixel that slot feeds; after a step the chain of a right pixel moves to
-// the next slot (left to right: k + 1; right to left: k - 1), so every step one chain is complete (slot
-// Dp-1, resp. slot 0) and is stored, and the rest are stored when the row ends. The left-to-right sweep
-// covers right pixels [mid - min - Dp + 1, w - 1 - min], the other one [-min - Dp + 1, mid - 1 - min]; the
-// epilogue takes the smaller key where both do.
+// Right WTA: candidate (x, k) belongs to right pixel xr = x - min - k. Each lane keeps, per slot, the
+// running minimum key of the right pixel that slot feeds; after every step the chains move by one slot
+// (left to right: k + 1; right to left: k - 1), so every step one chain is complete (slot Dp-1, resp.
+// slot 0) and is stored, and the rest are stored when the row ends. The left-to-right sweep covers right
+// pixels [mid - min - Dp + 1, w - 1 - min], the other one [-min - Dp + 1, mid - 1 - min]; the epilogue takes
+// the smaller key where both do.
 //
-// Best non-adjacent cost and the neighbours of the best (parabola): every lane stores its sums to shared
-// memory, the first lane of the segment reads cost(bk - 1) and cost(bk + 1) and raises the three slots
-// around bk, and a second reduction over the stored sums gives the best non-adjacent cost.
+// Best non-adjacent cost: the sums with the three slots around the best raised to >= 0xFFFD (per 16-bit
+// lane: t = min(k - bk + 1, 3) through the wrap, then max(t + 0xFFFD, sum)), reduced like the best. The
+// neighbours of the best (parabola) are read by the segment's first lane from the sums every lane stores
+// to shared memory.
+//
+// The step loop is unrolled by 2 steps (register pressure and instruction-cache footprint);
+// the strides along the row are compile-time, so loads use immediate offsets from pointers that move once
+// per unrolled iteration.
 
-constexpr int kSweepSmemWordsPerWarp = 2 * 32 * 8;  // two buffers of 32 lanes x 8 words (R <= 8)
+constexpr int kSweepSmemWordsPerWarp = 2 * 32 * 8;  // two buffers (step parity) of 32 lanes x R <= 8 words
 
-template <int R, int SEG, bool SLANT, bool PAD, int PF, bool FWD>
+template <int R, int SEG, bool SLANT, bool PAD, bool FWD>
 __device__ __forceinline__ void sweep_rows_dir(const SweepArgs& a, const uint32_t* __restrict__ p2t, uint32_t* __restrict__ wsm,
                                                int y, bool live, int seg, int sl) {
-    constexpr int NV = 2 * R, CW = R / 2;
+    constexpr int NV = 2 * R, CW = R / 2, Dp = SEG * NV, U = 2, PF = 2;
+    constexpr int dx = FWD ? 1 : -1;
     const int yc = live ? y : a.h - 1;
     const int k0 = sl * NV;
-    const int Dp = SEG * NV;
     const int mid = a.w / 2;
-    constexpr int dx = FWD ? 1 : -1;
     const int x0 = FWD ? 0 : a.w - 1;
     const int n1 = FWD ? mid : a.w - mid, n2 = a.w - n1;
     const uint32_t INF2 = splat2(0xFFFFu - static_cast<uint32_t>(a.p1)), P12 = splat2(static_cast<uint32_t>(a.p1));
@@ -343,39 +377,40 @@ __device__ __forceinline__ void sweep_rows_dir(const SweepArgs& a, const uint32_
     const long row = static_cast<long>(yc) * a.cpitch;
     const uint32_t* cl = a.census_l + row;
     const uint32_t* cr = a.census_r + row;
-    const uint8_t* grow = a.guide + static_cast<long>(yc) * a.w;
     const long prow = static_cast<long>(yc) * a.w;
     // The word entering the window at column x: lane 0 takes census_r(x - min) (left to right), lane
     // SEG-1 census_r(x - min - Dp + 1) (right to left).
     const int fresh_off = FWD ? -a.min_disp : -a.min_disp - Dp + 1;
 
+    // Stream pointers at the column of step `at`; a fetch of step at + i reads offset i * dx.
+    const uint32_t *pl, *pf;
+    const uint8_t *pg, *ps, *pt;
+    auto seek = [&](int at) {
+        const int x = x0 + at * dx;
+        pl = cl + x;
+        pf = cr + x + fresh_off;
+        pg = a.guide + prow + x;
+        ps = a.S + (prow + x) * Dp + k0;
+        pt = a.T + (prow + x) * Dp + k0;
+    };
+    auto move = [&](int steps) {
+        pl += steps * dx;
+        pf += steps * dx;
+        pg += steps * dx;
+        ps += steps * dx * Dp;
+        pt += steps * dx * Dp;
+    };
     int rI[PF];
     uint32_t rl[PF], rf[PF], rs[PF][CW], rt[PF][CW];
-    const uint32_t *fl, *ff;
-    const uint8_t *fg, *fs, *ft;
-    auto seek = [&](int s) {
-        const int x = x0 + s * dx;
-        fl = cl + x;
-        ff = cr + x + fresh_off;
-        fg = grow + x;
-        fs = a.S + (prow + x) * a.dp + k0;
-        ft = a.T + (prow + x) * a.dp + k0;
-    };
-    auto fetch = [&](int u, bool phase2) {
-        rI[u] = __ldg(fg);
-        rl[u] = __ldg(fl);
-        rf[u] = __ldg(ff);
+    auto fetch = [&](int u, int i, bool phase2) {  // ring slot u <- step at + i
+        rI[u] = __ldg(pg + i * dx);
+        rl[u] = __ldg(pl + i * dx);
+        rf[u] = __ldg(pf + i * dx);
         if (phase2) {
-            ld_chunk<NV, LD_CS>(fs, rs[u]);
-            ld_chunk<NV, LD_CG>(ft, rt[u]);
+            ld_chunk<NV, LD_CS>(ps + i * dx * Dp, rs[u]);
+            ld_chunk<NV, LD_CG>(pt + i * dx * Dp, rt[u]);
         }
-        fl += dx;
-        ff += dx;
-        fg += dx;
-        fs += dx * a.dp;
-        ft += dx * a.dp;
     };
-    // Window at the first column; afterwards advanced by one column per step.
     uint32_t win[NV];
 #pragma unroll
     for (int j = 0; j < NV; ++j) win[j] = __ldg(cr + x0 - a.min_disp - k0 - j);
@@ -392,14 +427,16 @@ __device__ __forceinline__ void sweep_rows_dir(const SweepArgs& a, const uint32_
             win[NV - 1] = sl == SEG - 1 ? fresh : t;
         }
     };
-    auto costs = [&](uint32_t lw, int x, uint32_t (&c)[R], uint32_t (&vm)[R], bool& edge) {
+    // Costs of column x; at columns where some slot's right pixel is outside the row, vm marks the valid
+    // slots (0xFFFF lanes) and the others take the invalid cost.
+    auto costs = [&](uint32_t lw, int x, uint32_t (&c)[R], uint32_t (&vm)[R]) -> bool {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const uint32_t ca = static_cast<uint32_t>(__popc(lw ^ win[r]));
             const uint32_t cb = static_cast<uint32_t>(__popc(lw ^ win[r + R]));
             c[r] = ca | (cb << 16);
         }
-        edge = x < x_in_lo || x > x_in_hi;  // the same for every lane of the warp (one column per warp)
+        const bool edge = x < x_in_lo || x > x_in_hi;  // one column per warp: uniform
         if (edge) {
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -409,69 +446,75 @@ __device__ __forceinline__ void sweep_rows_dir(const SweepArgs& a, const uint32_
                 c[r] = (c[r] & vm[r]) | (inv2 & ~vm[r]);
             }
         }
+        return edge;
     };
 
-    uint32_t v[R], pm2 = 0, c[R], vm[R], w[CW];
+    uint32_t v[R], pm2 = 0, vm[R];
     int last = 0;
-    bool edge = false;
+    int x = x0;
+    // ---- phase 1: the first half of the row, path values to T
     seek(0);
 #pragma unroll
     for (int u = 0; u < PF; ++u)
-        if (u < n1) fetch(u, false);
-    int x = x0;
-    for (int base = 0; base < n1; base += PF) {
+        if (u < n1) fetch(u, u, false);
+    for (int base = 0; base < n1; base += U) {
 #pragma unroll
-        for (int u = 0; u < PF; ++u) {
+        for (int u = 0; u < U; ++u) {
             const int s = base + u;
             if (s >= n1) break;
-            if (s > 0) advance(rf[u]);
-            costs(rl[u], x, c, vm, edge);
-            const uint32_t p2v = sw_p2(p2t, rI[u], last);
-            if (s + PF < n1) fetch(u, false);
+            if (s > 0) advance(rf[u % PF]);
+            uint32_t c[R];
+            costs(rl[u % PF], x, c, vm);
+            const uint32_t p2v = sw_p2(p2t, rI[u % PF], last);
+            if (s + PF < n1) fetch(u % PF, u + PF, false);
             if (s == 0) sw_first<R, SEG, PAD>(v, pm2, c, INF2, pad, seg);
             else sw_step<R, SEG, SLANT, PAD>(v, pm2, c, pm2 + p2v, INF2, P12, pad, sl, seg);
             if (live) {
+                uint32_t w[CW];
                 sw_pack<R>(v, w);
-                st_chunk<NV, false>(a.T + (prow + x) * a.dp + k0, w);
+                st_chunk<NV, false>(a.T + (prow + x) * Dp + k0, w);
             }
             x += dx;
         }
+        move(U);
     }
     sw_block_barrier();  // the other direction's first half is in T
 
+    // ---- phase 2: the second half, with the 4-direction sums and the WTA
     uint16_t* rk = a.rk + (FWD ? 0 : static_cast<size_t>(a.w) * a.h) + prow;
     uint2* rec = a.rec + prow;
     uint32_t acc[R];  // running right-WTA keys of the right pixels x - min - (k0 + slot)
 #pragma unroll
     for (int r = 0; r < R; ++r) acc[r] = 0xFFFFFFFFu;
-    // Shared memory of this warp: two buffers (step parity) of 32 lanes x (two 16-byte quarters), so that
-    // each 128-bit store of a quarter-warp is contiguous.
     const int lane = threadIdx.x & 31;
-    const int segbase = seg * SEG;
+    uint16_t* hb = reinterpret_cast<uint16_t*>(wsm);
     seek(n1);
 #pragma unroll
     for (int u = 0; u < PF; ++u)
-        if (u < n2) fetch(u, true);
-    for (int base = 0; base < n2; base += PF) {
+        if (u < n2) fetch(u, u, true);
+    for (int base = 0; base < n2; base += U) {
 #pragma unroll
-        for (int u = 0; u < PF; ++u) {
+        for (int u = 0; u < U; ++u) {
             const int s = base + u;
             if (s >= n2) break;
-            if (n1 + s > 0) advance(rf[u]);
-            costs(rl[u], x, c, vm, edge);
-            const uint32_t p2v = sw_p2(p2t, rI[u], last);
-            uint32_t tot[R], t2[R];
-            sw_unpack<R>(rs[u], tot);
-            sw_unpack<R>(rt[u], t2);
-            if (s + PF < n2) fetch(u, true);
+            if (n1 + s > 0) advance(rf[u % PF]);
+            uint32_t c[R];
+            const bool edge = costs(rl[u % PF], x, c, vm);
+            const uint32_t p2v = sw_p2(p2t, rI[u % PF], last);
             if (n1 == 0 && s == 0) sw_first<R, SEG, PAD>(v, pm2, c, INF2, pad, seg);
             else sw_step<R, SEG, SLANT, PAD>(v, pm2, c, pm2 + p2v, INF2, P12, pad, sl, seg);
-            // The reference's 4-direction sum and the keys (sum << 7 | k); candidates outside the row or
-            // beyond nd get 0xFFFF.
-            uint32_t key[R];
+            // The reference's 4-direction sum S + T + L (S <= 254 and T <= 127 per byte, no overflow) and the
+            // keys (sum << 7 | k); candidates outside the row or beyond nd get 0xFFFF.
+            uint32_t tot[R], key[R];
+#pragma unroll
+            for (int i = 0; i < CW; ++i) {
+                tot[2 * i] = prmt(rs[u % PF][i], 0u, 0x4240) + prmt(rt[u % PF][i], 0u, 0x4240);
+                tot[2 * i + 1] = prmt(rs[u % PF][i], 0u, 0x4341) + prmt(rt[u % PF][i], 0u, 0x4341);
+            }
+            if (s + PF < n2) fetch(u % PF, u + PF, true);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                tot[r] += t2[r] + (PAD ? (v[r] & ~pad[r]) : v[r]);
+                tot[r] += PAD ? (v[r] & ~pad[r]) : v[r];
                 key[r] = tot[r] * (1u << kSweepKeyBits) + (kbase2 + static_cast<uint32_t>(r) * 0x00010001u);
                 if (PAD) {
                     key[r] |= pad[r];
@@ -485,99 +528,83 @@ __device__ __forceinline__ void sweep_rows_dir(const SweepArgs& a, const uint32_
                     tot[r] |= ~vm[r];
                 }
             }
-            // Left WTA: the segment's smallest key.
-            uint32_t km = key[0];
-#pragma unroll
-            for (int r = 1; r < R; ++r) km = vmin2(km, key[r]);
-            const uint32_t kmin = sw_seg_min2<SEG>(km, seg) & 0xFFFFu;
-            // Right WTA chains.
+            // Right WTA chains: add this column's candidates, store the completed chain, shift.
 #pragma unroll
             for (int r = 0; r < R; ++r) acc[r] = vmin2(acc[r], key[r]);
             if constexpr (FWD) {
                 const int xr = x - a.min_disp - (Dp - 1);
                 if (live && sl == SEG - 1 && static_cast<unsigned>(xr) < static_cast<unsigned>(a.w))
                     rk[xr] = static_cast<uint16_t>(acc[R - 1] >> 16);
+                uint32_t t = __shfl_up_sync(kFull, acc[R - 1], 1, SEG);
+                t = sl == 0 ? 0xFFFFFFFFu : t;
+                const uint32_t a0 = prmt(t, acc[R - 1], 0x5432);
+#pragma unroll
+                for (int r = R - 1; r > 0; --r) acc[r] = acc[r - 1];
+                acc[0] = a0;
             } else {
                 const int xr = x - a.min_disp;
                 if (live && sl == 0 && static_cast<unsigned>(xr) < static_cast<unsigned>(a.w))
                     rk[xr] = static_cast<uint16_t>(acc[0]);
-            }
-            if (s + 1 < n2) {  // shift the chains by one disparity (the last step keeps them for the flush)
-                if constexpr (FWD) {
-                    uint32_t t = __shfl_up_sync(kFull, acc[R - 1], 1, SEG);
-                    t = sl == 0 ? 0xFFFFFFFFu : t;
-                    const uint32_t a0 = prmt(t, acc[R - 1], 0x5432);
+                uint32_t t = __shfl_down_sync(kFull, acc[0], 1, SEG);
+                t = sl == SEG - 1 ? 0xFFFFFFFFu : t;
+                const uint32_t ae = prmt(acc[0], t, 0x5432);
 #pragma unroll
-                    for (int r = R - 1; r > 0; --r) acc[r] = acc[r - 1];
-                    acc[0] = a0;
-                } else {
-                    uint32_t t = __shfl_down_sync(kFull, acc[0], 1, SEG);
-                    t = sl == SEG - 1 ? 0xFFFFFFFFu : t;
-                    const uint32_t ae = prmt(acc[0], t, 0x5432);
-#pragma unroll
-                    for (int r = 0; r < R - 1; ++r) acc[r] = acc[r + 1];
-                    acc[R - 1] = ae;
-                }
+                for (int r = 0; r < R - 1; ++r) acc[r] = acc[r + 1];
+                acc[R - 1] = ae;
             }
-            // Best non-adjacent cost and the neighbours of the best, through shared memory.
+            // Left WTA: the segment's smallest key (key[] is reduced in place).
+            const uint32_t kmin = sw_seg_min2<SEG>(sw_tree_min<R>(key), seg) & 0xFFFFu;
+            const int bk = static_cast<int>(kmin & ((1u << kSweepKeyBits) - 1));
+            // The sums to shared memory (lane l's R words at l * R) for the neighbours of the best.
             uint32_t* buf = wsm + (u & 1) * (32 * 8);
             {
-                uint4* q0 = reinterpret_cast<uint4*>(buf) + lane;
-                *q0 = make_uint4(tot[0], tot[1], tot[2], tot[3]);
-                if constexpr (R == 8) *(reinterpret_cast<uint4*>(buf + 32 * 4) + lane) = make_uint4(tot[4], tot[5], tot[6], tot[7]);
-                else *(reinterpret_cast<uint2*>(buf + 32 * 4) + lane) = make_uint2(tot[4], tot[5]);
-            }
-            __syncwarp();
-            const int bk = static_cast<int>(kmin & ((1u << kSweepKeyBits) - 1));
-            const bool found = kmin < kSweepNoKey;
-            // u16 address of disparity k within the segment's stored sums
-            auto haddr = [&](int k) {
-                const int ln = segbase + k / NV, j = k % NV, rr = j % R, hf = j / R;
-                const int word = rr < 4 ? (ln * 4 + rr) : (32 * 4 + ln * (R - 4) + (rr - 4));
-                return word * 2 + hf;
-            };
-            uint16_t* hb = reinterpret_cast<uint16_t*>(buf);
-            uint32_t cm = 0, cp = 0;
-            if (sl == 0 && found) {
-                cm = hb[haddr(max(bk - 1, 0))];
-                cp = hb[haddr(min(bk + 1, a.nd - 1))];
-            }
-            __syncwarp();
-            if (sl == 0 && found) {
-                hb[haddr(bk)] = 0xFFFFu;
-                if (bk > 0) hb[haddr(bk - 1)] = 0xFFFFu;
-                if (bk + 1 < Dp) hb[haddr(bk + 1)] = 0xFFFFu;
-            }
-            __syncwarp();
-            uint32_t m2;
-            {
-                const uint4 q0 = *(reinterpret_cast<const uint4*>(buf) + lane);
-                m2 = vmin2(vmin2(q0.x, q0.y), vmin2(q0.z, q0.w));
-                if constexpr (R == 8) {
-                    const uint4 q1 = *(reinterpret_cast<const uint4*>(buf + 32 * 4) + lane);
-                    m2 = vmin2(m2, vmin2(vmin2(q1.x, q1.y), vmin2(q1.z, q1.w)));
+                uint32_t* q = buf + lane * R;  // 16-byte aligned when R % 4 == 0, else 8-byte aligned
+                if constexpr (R % 4 == 0) {
+#pragma unroll
+                    for (int i = 0; i < R / 4; ++i)
+                        reinterpret_cast<uint4*>(q)[i] = make_uint4(tot[4 * i], tot[4 * i + 1], tot[4 * i + 2], tot[4 * i + 3]);
                 } else {
-                    const uint2 q1 = *(reinterpret_cast<const uint2*>(buf + 32 * 4) + lane);
-                    m2 = vmin2(m2, vmin2(q1.x, q1.y));
+#pragma unroll
+                    for (int i = 0; i < R / 2; ++i) reinterpret_cast<uint2*>(q)[i] = make_uint2(tot[2 * i], tot[2 * i + 1]);
                 }
             }
-            const uint32_t second = sw_seg_min2<SEG>(m2, seg) & 0xFFFFu;
-            if (live && sl == 0) rec[x] = make_uint2(kmin | (second << 16), (cm & 0xFFFFu) | (cp << 16));
+            // Best non-adjacent cost: slots within one of bk raised to >= 0xFFFD (tot[] reduced in place).
+            const uint32_t kc = vadd2(kbase2, splat2((1u - static_cast<uint32_t>(bk)) & 0xFFFFu));
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const uint32_t t = __viaddmin_u16x2(kc, static_cast<uint32_t>(r) * 0x00010001u, 0x00030003u);
+                tot[r] = __viaddmax_u16x2(t, 0xFFFDFFFDu, tot[r]);
+            }
+            const uint32_t second = sw_seg_min2<SEG>(sw_tree_min<R>(tot), seg) & 0xFFFFu;
+            __syncwarp();
+            if (live && sl == 0) {
+                // u16 index of disparity k within the segment: lane k / NV, register (k % NV) % R, half (k % NV) / R.
+                // k is clamped into [0, nd): without any candidate (every key 0xFFFF) bk is not a disparity, and
+                // the record is not used.
+                auto hidx = [&](int k) {
+                    k = min(max(k, 0), a.nd - 1);
+                    const int j = k % NV;
+                    return (u & 1) * 512 + ((seg * SEG + k / NV) * R + j % R) * 2 + j / R;
+                };
+                const uint32_t cm = hb[hidx(bk - 1)];
+                const uint32_t cp = hb[hidx(bk + 1)];
+                rec[x] = make_uint2(kmin | (second << 16), cm | (cp << 16));
+            }
             x += dx;
         }
+        move(U);
     }
-    // Flush: every slot's chain is complete (no later column feeds it).
+    // Flush: every chain is complete (no later column feeds it). The chains were shifted after the last
+    // step, so slot k holds the right pixel of slot k - dx at the last column.
     if (live) {
         const int xl = FWD ? a.w - 1 : 0;  // the last column of the sweep
 #pragma unroll
         for (int r = 0; r < R; ++r) {
 #pragma unroll
             for (int hf = 0; hf < 2; ++hf) {
-                const int j = r + hf * R;
-                const int k = k0 + j;
-                if (FWD && k == Dp - 1) continue;  // stored at the last step
-                if (!FWD && k == 0) continue;
-                const int xr = xl - a.min_disp - k;
+                const int k = k0 + r + hf * R;
+                if (FWD ? k == 0 : k == Dp - 1) continue;  // shifted in: no chain
+                const int xr = xl - a.min_disp - (k - dx);
                 if (static_cast<unsigned>(xr) < static_cast<unsigned>(a.w))
                     rk[xr] = static_cast<uint16_t>(hf ? (acc[r] >> 16) : acc[r]);
             }
@@ -645,8 +672,8 @@ __device__ __forceinline__ void sweep_rows_body(const SweepArgs& a, const uint32
     const int y = bx * rows + wi * LPW + seg;
     const bool live = y < a.h;
     uint32_t* wsm = smem + warp * kSweepSmemWordsPerWarp;
-    if (fwd) sweep_rows_dir<R, SEG, SLANT, PAD, PF, true>(a, p2t, wsm, y, live, seg, sl);
-    else sweep_rows_dir<R, SEG, SLANT, PAD, PF, false>(a, p2t, wsm, y, live, seg, sl);
+    if (fwd) sweep_rows_dir<R, SEG, SLANT, PAD, true>(a, p2t, wsm, y, live, seg, sl);
+    else sweep_rows_dir<R, SEG, SLANT, PAD, false>(a, p2t, wsm, y, live, seg, sl);
     __syncthreads();  // records and right-WTA keys of the block's rows are stored
     sweep_rows_epilogue(a, bx * rows, rows, SEG * 2 * R);
 }
