@@ -178,8 +178,7 @@ def cpu_reference_sample(pairs, budget_s=20.0, max_frames=8):
 def run_reference(args, world, rank):
     if rank != 0:
         return 0
-    from open_source_einstar_b200 import synth
-    pairs = [synth.raw_objects_pair(seed=1000 + i, device="cpu") for i in range(2)]
+    pairs = make_frames(2, replica_seed0(rank), "cpu")  # the scenes the GPU arm's first frames render
     from oracle.oracle import Ref
     ref = Ref()
     for i in range(args.warmup):
@@ -253,13 +252,21 @@ def run_serving(args, world, rank, local):
     """Poisson arrivals at each rate for --duration seconds through StereoServer (ds_server_*): latency
     p50/p99/p99.9 from submit to results in host memory, beside frames/s. One GPU; replicas beyond."""
     import torch
+    torch.cuda.set_device(local)
+    line = serving_line(torch.device("cuda", local), args.rates, args.duration, args.slots, world, rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def serving_line(dev, rates, duration, slots, world=1, rank=0):
+    """The serving workload's JSON line (configuration 4) on device `dev`."""
+    import torch
     from open_source_einstar_b200 import RectifiedGeometry, RemapTable
     from open_source_einstar_b200.serving import StereoServer, latency_summary, poisson_arrivals, replay
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
     cal = serving_calibrations(dev)
     reqs = serving_requests(cal, 512, seed=11 + rank)
-    srv = StereoServer(volume_budget_bytes=40 << 30, max_slots=args.slots)
+    srv = StereoServer(volume_budget_bytes=40 << 30, max_slots=slots)
     for ci, (r, s, w, h, pr) in enumerate(cal):
         (lx, ly), (rx, ry) = pr.maps
         srv.add_calibration(ci, RemapTable(lx, ly), RemapTable(rx, ry), w, h,
@@ -268,12 +275,12 @@ def run_serving(args, world, rank, local):
     for ci, (r, s, w, h, pr) in enumerate(cal[:3]):  # every (size, D) kind, all slots, before the clock starts
         for d in SERVE_D:
             srv.reserve(w, h, StereoParams(sgm=SgmParams(min_disparity=pr.min_disparity, num_disparities=d)), ci,
-                        args.slots)
+                        slots)
     replay(srv, reqs, poisson_arrivals(480.0, 0.5, seed=99))  # warm-up
-    clk = ClockSampler(local).__enter__()
+    clk = ClockSampler(dev.index or 0).__enter__()
     results = []
-    for k, rate in enumerate(args.rates):
-        arr = poisson_arrivals(rate, args.duration, seed=100 + k)
+    for k, rate in enumerate(rates):
+        arr = poisson_arrivals(rate, duration, seed=100 + k)
         comps, wall = replay(srv, reqs, arr)
         bad = [c for c in comps if not c.ok]
         if bad:
@@ -281,27 +288,25 @@ def run_serving(args, world, rank, local):
         lat = [c.latency_ms for c in comps]
         pxd = sum(reqs[c.tag % len(reqs)]["px_d"] for c in comps)
         summ = latency_summary(lat, wall)
-        summ.update({"rate_hz": rate, "seconds": args.duration, "gpix_disp_per_s": pxd / wall / 1e9,
+        summ.update({"rate_hz": rate, "seconds": duration, "gpix_disp_per_s": pxd / wall / 1e9,
                      "gpu_ms_p50": float(np.percentile([c.gpu_ms for c in comps], 50)),
                      "queue_ms_p99": float(np.percentile([c.queue_ms for c in comps], 99))})
         results.append(summ)
     clk.__exit__(None, None, None)
     st = srv.stats()
     srv.close()
-    if rank == 0:
-        line = {"metric": "serving frame latency p50/p99/p99.9 (ms) beside frames/s, Poisson arrivals",
-                "workload": "serving", "unit": "ms", "higher_is_better": False, "n_gpus": world,
-                "value": max(r["p99_ms"] for r in results), "value_is": "worst p99 latency over the rates",
-                "rates": results, "dtype": "u8", "data": "synthetic",
-                "config": {"workload": "Poisson arrivals; sizes 70 % 1280x1024, 20 % 960x768, 10 % 640x512 (raw pairs, "
-                                       "GPU remap); D in {96, 128}; 4 resident synthetic rigs x 3 sizes; 40 GB volume "
-                                       "budget; latency = submit -> u16 disparity + depth in pinned host memory",
-                           "slots": args.slots, "parallelism": f"replicas x{world}"},
-                "server": {"peak_running": st["peak_running"], "slots": st["slots"],
-                           "volume_bytes": st["volume_bytes"], "device_bytes": st["device_bytes"]},
-                "clocks": clk.summary()}
-        print(json.dumps(line), flush=True)
-    return 0
+    line = {"metric": "serving frame latency p50/p99/p99.9 (ms) beside frames/s, Poisson arrivals",
+            "workload": "serving", "unit": "ms", "higher_is_better": False, "n_gpus": world,
+            "value": max(r["p99_ms"] for r in results), "value_is": "worst p99 latency over the rates",
+            "rates": results, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": "Poisson arrivals; sizes 70 % 1280x1024, 20 % 960x768, 10 % 640x512 (raw pairs, "
+                                   "GPU remap); D in {96, 128}; 4 resident synthetic rigs x 3 sizes; 40 GB volume "
+                                   "budget; latency = submit -> u16 disparity + depth in pinned host memory",
+                       "slots": slots, "parallelism": f"replicas x{world}"},
+            "server": {"peak_running": st["peak_running"], "slots": st["slots"],
+                       "volume_bytes": st["volume_bytes"], "device_bytes": st["device_bytes"]},
+            "clocks": clk.summary()}
+    return line
 
 
 # ---- uneven batch: 64 rectified pairs of three sizes and four disparity ranges in one graph replay -----------
@@ -310,11 +315,20 @@ def run_batch64(args, world, rank, local):
     calibration) as one StereoBatch graph replay with autotuned kernels and schedule, against the same
     pairs launched per frame (one handle per pair, back to back on one stream). Bit-exact check first."""
     import torch
+    torch.cuda.set_device(local)
+    line = batch64_line(torch.device("cuda", local), args.steps, args.warmup, world, rank, tune_schedule=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def batch64_line(dev, steps, warmup, world=1, rank=0, tune_schedule=True):
+    """The 64-pair uneven batch's JSON line (configuration 3) on device `dev`; without tune_schedule the
+    library's default (micro_batch, branches) is used."""
+    import torch
     from open_source_einstar_b200 import (CudaStereo, PairDesc, RectifiedGeometry, SgmParams, StereoBatch, StereoParams,
                                           synth)
     from open_source_einstar_b200.autotune import Autotuner, FrameKind, tune_batch_schedule
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
     pairs = synth.batch_pairs(64, seed=rank, device=dev)
     tuner = Autotuner()
     descs, handles, ins, outs = [], [], [], []
@@ -357,9 +371,13 @@ def run_batch64(args, world, rank, local):
         return e0.elapsed_time(e1)
 
     bouts = [{k: torch.empty_like(v) for k, v in o.items()} for o in outs]
-    (mb, br), sched = tune_batch_schedule(make_batch, time_run, len(descs))
+    if tune_schedule:
+        (mb, br), sched = tune_batch_schedule(make_batch, time_run, len(descs))
+    else:
+        mb, br, sched = 0, 0, {}
     batch = make_batch(mb, br)
-    for _ in range(args.warmup):
+    mb, br = batch.micro_batch, batch.branches
+    for _ in range(warmup):
         per_frame()
         batch.run(stream=stream)
     torch.cuda.synchronize(dev)
@@ -367,24 +385,24 @@ def run_batch64(args, world, rank, local):
         if not (torch.equal(o["disparity_u16"], bo["disparity_u16"]) and torch.equal(o["depth"], bo["depth"])):
             raise SystemExit(f"pair {i}: batched and per-pair outputs differ")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clk = ClockSampler(local).__enter__()
+    clk = ClockSampler(dev.index or 0).__enter__()
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         per_frame()
     e1.record(stream)
     e1.synchronize()
-    pf_ms = e0.elapsed_time(e1) / args.steps
+    pf_ms = e0.elapsed_time(e1) / steps
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         batch.run(stream=stream)
     e1.record(stream)
     e1.synchronize()
-    b_ms = e0.elapsed_time(e1) / args.steps
+    b_ms = e0.elapsed_time(e1) / steps
     clk.__exit__(None, None, None)
     hbm, hbm_kind = peaks()
     line = {"metric": "batched SGM Gpix*disp/s, 64 uneven pairs in one graph replay vs per-frame launches",
             "workload": "batch64", "value": px_d / (b_ms * 1e-3) / 1e9, "unit": UNIT, "higher_is_better": True,
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": b_ms,
+            "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": b_ms,
             "per_frame": {"value": px_d / (pf_ms * 1e-3) / 1e9, "ms_per_step": pf_ms},
             "batched_over_per_frame": pf_ms / b_ms,
             "pipeline_frac": formula / (b_ms * 1e-3) / 1e9 / hbm, "peak_gbs": hbm, "peak_kind": hbm_kind,
@@ -401,9 +419,8 @@ def run_batch64(args, world, rank, local):
     batch.close()
     for s in handles:
         s.close()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    return 0
+    torch.cuda.set_stream(torch.cuda.default_stream(dev))
+    return line
 
 
 # ---- offline re-depth: a raw recording in batches of 128 at D=256, 8 paths, u16 path values -----------------
@@ -614,6 +631,33 @@ def run_frontend(args, world, rank, local):
     return 0
 
 
+def plugin_leg(stereo, pairs, calls, warmup=3):
+    """End to end through the drop-in call, one frame per call as the scanner frontend makes it
+    (StereoFrontend::process -> compute_raw, stereo_frontend.cpp:317): CudaStereo.compute_raw, i.e.
+    ds_compute_raw, with the raw pair in pinned host memory and the u16 disparity + depth written back to
+    pinned host memory; the call returns when they are there. Host-clock latency per call and throughput."""
+    from open_source_einstar_b200 import StereoResult
+    from open_source_einstar_b200.serving import pinned_copy, pinned_empty
+    host = [(pinned_copy(p.left), pinned_copy(p.right)) for p in pairs[:4]]
+    res = StereoResult(disparity=None, confidence=None, disparity_u16=pinned_empty((H, W), np.uint16),
+                       depth=pinned_empty((H, W), np.float32))
+    for i in range(warmup):
+        stereo.compute_raw(*host[i % len(host)], out=res)
+    lat = []
+    t0 = time.perf_counter()
+    for i in range(calls):
+        t = time.perf_counter()
+        stereo.compute_raw(*host[i % len(host)], out=res)
+        lat.append((time.perf_counter() - t) * 1e3)
+    total = time.perf_counter() - t0
+    return {"value": calls * PX_D / total / 1e9, "unit": UNIT, "calls": calls,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "max": float(max(lat))},
+            "h2d_bytes_per_call": 2 * W * H, "d2h_bytes_per_call": W * H * (2 + 4),
+            "api": "CudaStereo.compute_raw (ds_compute_raw): raw pair from pinned host memory in, u16 disparity + f32 "
+                   "depth in pinned host memory out, one frame per synchronous call; host clock"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -631,6 +675,9 @@ def main():
     ap.add_argument("--slots", type=int, default=6, help="serving: frames on the GPU at once")
     ap.add_argument("--recording-frames", type=int, default=256, help="offline: frames of the synthetic recording")
     ap.add_argument("--offline-batch", type=int, default=128, help="offline: frames per batch")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default line without the serving and 64-pair batch summaries (single-GPU runs carry them)")
+    ap.add_argument("--extras-duration", type=float, default=3.0, help="serving summary: seconds of arrivals per rate")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -765,6 +812,7 @@ def main():
         if not np.array_equal(e2e_u16[n_e2e - B + j], outs[j]["disparity_u16"].cpu().numpy().view(np.uint16)):
             raise SystemExit("end-to-end outputs differ from the per-frame path")
     off.close()
+    plug = plugin_leg(s, pairs, max(16, 2 * args.steps))
     clk.__exit__(None, None, None)
 
     # ---- roofline of the dominant kernel: the SGM path launch (k_paths), one frame per launch, timed by the
@@ -823,11 +871,22 @@ def main():
                     "api": "OfflineRedepth (StereoBatch graph replays, ds_batch_run) with every step's raw pairs copied in "
                            "from pinned host memory and its u16 disparity + depth copied out; steps double-buffered",
                     "steps": e2e_steps},
+            "e2e_plugin": plug,
             "gpu_launches": int(launches), "clocks": clk.summary()}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     batch.close()
     s.close()
+    if world == 1 and not args.no_extras:
+        # configurations 4 and 3 on the same box: the request server under Poisson arrivals (a shorter run per
+        # rate than --workload serving) and the 64-pair uneven batch against per-frame launches
+        srv = serving_line(dev, args.rates, args.extras_duration, args.slots)
+        line["serving"] = {"rates": srv["rates"], "worst_p99_ms": srv["value"], "slots": srv["config"]["slots"],
+                           "seconds_per_rate": args.extras_duration, "clocks": srv["clocks"]}
+        b64 = batch64_line(dev, 3, 2, tune_schedule=False)
+        line["batch64"] = {k: b64[k] for k in ("value", "unit", "ms_per_step", "per_frame", "batched_over_per_frame",
+                                               "pipeline_frac", "schedule", "launches_per_run", "kernels", "clocks")}
+        line["batch64"]["bit_exact_vs_per_frame"] = True  # batch64_line stops the run otherwise
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0

@@ -349,7 +349,7 @@ DS_API int ds_set_blob_params(ds_handle* handle, const ds_blob_params* params);
  * stereo (MetalStereo::compute_frame with FrameRequest::marker_blobs). */
 DS_API int ds_compute_raw_blobs(ds_handle* handle, const uint8_t* raw_left, const uint8_t* raw_right, ptrdiff_t stride,
                                 const ds_outputs* out, ds_blob_boxes* blobs);
-/* MetalStereo::compute_frame (metal_stereo.hpp:88-91 with FrameRequest / FrameOutputs, :41-58), the call the
+/* MetalStereo::compute_frame (metal_stereo.hpp:92-95 with FrameRequest / FrameOutputs, :41-58), the call the
  * scanner frontend makes per frame (libs/pipeline/src/stereo_frontend.cpp:302-328): raw pair in; the
  * frame's points, normals and weights (ds_disparity_to_points with the handle's point parameters and the
  * default ds_point_params otherwise) written to the caller's device buffers and left there; optional host
@@ -371,6 +371,14 @@ typedef struct ds_frame_outputs {
 } ds_frame_outputs;
 DS_API int ds_compute_frame(ds_handle* handle, const uint8_t* raw_left, const uint8_t* raw_right, ptrdiff_t stride,
                             const ds_frame_request* request, ds_frame_outputs* out);
+/* MetalStereo::compute_frame_raw (metal_stereo.hpp:86-90, metal_stereo.cpp:251-275): raw pair (host, rows `stride`
+ * bytes apart) -> rectified -> stereo (with the handle's filters) -> points, normals and weights written to the
+ * caller's device buffers (W*H float4, float4, float; required) and left there. rect_left / rect_right: host
+ * W x H buffers for the rectified pair, or NULL. Needs ds_set_rectification and ds_set_point_params (the
+ * reference's errors). Returns when the frame has finished. */
+DS_API int ds_compute_frame_raw(ds_handle* handle, const uint8_t* raw_left, const uint8_t* raw_right, ptrdiff_t stride,
+                                float* points_xyzw, float* normals_xyzw, float* weights, uint8_t* rect_left,
+                                uint8_t* rect_right);
 
 /* The blob search alone on one host image of any size (width x height, rows `stride` bytes apart):
  * up to `capacity` boxes, `found` = candidates that passed. Needs ds_set_blob_params. */
@@ -457,7 +465,9 @@ DS_API int ds_server_get_stats(ds_server* server, ds_server_stats* out);
  * (two W x H census images of 4- or 8-byte words, plus P paths x W x H x disparities of 1- or 2-byte path
  * values; about 320 x 240 at 32 disparities and 4 paths fits) is rejected with DS_INVALID_ARGUMENT and a
  * message giving the bytes needed. The first call on each device looks up the array's device address
- * (with that device current) and should come before any stream capture. Calls share the array: calls
+ * (with that device current) and should come before any stream capture. The address is kept per device
+ * for the life of the process: calls must run in the device's primary context (the CUDA runtime's, which
+ * is what cudaSetDevice makes current), and not after a cudaDeviceReset. Calls share the array: calls
  * whose work overlaps on the GPU (other streams, other threads) race and must be serialised by the
  * caller. Errors: ds_last_global_error(). */
 DS_API int ds_sgm_disparity_noalloc(const uint8_t* left, const uint8_t* right, int width, int height,

@@ -156,6 +156,7 @@ SIGNATURES = {
     "ds_set_blob_params": (_i, [_vp, C.POINTER(BlobParamsC)]),
     "ds_compute_raw_blobs": (_i, [_vp, _vp, _vp, C.c_ssize_t, C.POINTER(OutputsC), C.POINTER(BlobBoxesC)]),
     "ds_compute_frame": (_i, [_vp, _vp, _vp, C.c_ssize_t, C.POINTER(FrameRequestC), C.POINTER(FrameOutputsC)]),
+    "ds_compute_frame_raw": (_i, [_vp, _vp, _vp, C.c_ssize_t, _vp, _vp, _vp, _vp, _vp]),
     "ds_find_blobs": (_i, [_vp, _vp, _i, _i, C.c_ssize_t, _vp, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "ds_server_create": (_i, [C.POINTER(ServerOptionsC), C.POINTER(_vp)]),
     "ds_server_destroy": (None, [_vp]),

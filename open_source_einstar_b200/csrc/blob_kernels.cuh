@@ -140,7 +140,8 @@ static __global__ void k_blob_select(BlobArgs a) {
     if (static_cast<int>(x0) - m < bd || static_cast<int>(y0) - m < bd || static_cast<int>(x1) + m >= a.w - bd ||
         static_cast<int>(y1) + m >= a.h - bd)
         return;
-    // Ellipse of the blob from its second moments (a filled ellipse has variance (axis / 2)^2).
+    // Semi-axes from the eigenvalues of the central moment matrix: spread uniformly over an ellipse, the pixels
+    // have variance s^2 / 4 along a semi-axis of length s, so s = 2 sqrt(lambda).
     const int* mo = a.mom + 5 * static_cast<size_t>(i);
     const float fn = static_cast<float>(px);
     const float mx = __fdiv_rn(static_cast<float>(mo[0]), fn), my = __fdiv_rn(static_cast<float>(mo[1]), fn);
@@ -151,7 +152,7 @@ static __global__ void k_blob_select(BlobArgs a) {
     const float tr = __fmul_rn(0.5f, __fadd_rn(cxx, cyy));
     const float det = __fsqrt_rn(fmaxf(0.0f, __fadd_rn(__fmul_rn(__fmul_rn(0.25f, dxy), dxy), __fmul_rn(cxy, cxy))));
     const float l1 = __fadd_rn(tr, det), l2 = fmaxf(__fsub_rn(tr, det), 0.0625f);
-    // + half a pixel: the threshold edge sits inside the half-level contour
+    // + 0.5: the pixels above the threshold stop about half a pixel short of the blob's true outline
     const float ea = __fadd_rn(__fmul_rn(2.0f, __fsqrt_rn(fmaxf(l1, 0.0f))), 0.5f), eb = __fadd_rn(__fmul_rn(2.0f, __fsqrt_rn(l2)), 0.5f);
     if (__fdiv_rn(ea, eb) > __fmul_rn(a.max_axis_ratio, 1.2f)) return;
     // Major-axis direction (angle th = atan2(2 cxy, cxx - cyy) / 2): cos th = sqrt((1 + cos 2th) / 2),
@@ -166,7 +167,7 @@ static __global__ void k_blob_select(BlobArgs a) {
         if (s2 < 0.0f) st = -st;
     }
     const float cx = __fadd_rn(static_cast<float>(i % a.w), mx), cy = __fadd_rn(static_cast<float>(i / a.w), my);
-    // Background: the 4th lowest of 16 samples on the surface outside the sticker (2.2x the disc).
+    // Local background level: the 4th smallest grey value among 16 points of an ellipse 2.2 times the blob's.
     float bg[16];
     const float bu = __fmul_rn(2.2f, ea), bv = __fmul_rn(2.2f, eb);
 #pragma unroll
@@ -181,7 +182,8 @@ static __global__ void k_blob_select(BlobArgs a) {
                 bg[q] = t;
             }
     const float level = __fadd_rn(bg[3], __fmul_rn(a.ring_contrast, __fsub_rn(static_cast<float>(pk), bg[3])));
-    // The sticker's dark ring must surround the disc (laser speckle dots sit among bright neighbours).
+    // A retro-reflective marker is framed by a dark annulus; a projected speckle dot has bright dots around it.
+    // Reject the blob when too many points of the ring_scale ellipse are brighter than the level.
     const float ru = __fmul_rn(a.ring_scale, ea), rv = __fmul_rn(a.ring_scale, eb);
     int bright = 0;
 #pragma unroll

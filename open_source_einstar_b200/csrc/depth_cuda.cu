@@ -1380,6 +1380,20 @@ DS_API int ds_compute_frame(ds_handle* h, const uint8_t* left, const uint8_t* ri
     return guarded(h, [&] { return run_host(h, left, right, stride, &out->host, true, &fx); });
 }
 
+DS_API int ds_compute_frame_raw(ds_handle* h, const uint8_t* left, const uint8_t* right, ptrdiff_t stride, float* points_xyzw,
+                                float* normals_xyzw, float* weights, uint8_t* rect_left, uint8_t* rect_right) {
+    if (!h) return DS_INVALID_ARGUMENT;
+    if (!h->have_points) return h->fail(DS_INVALID_ARGUMENT, "set_point_params() not called");  // metal_stereo.cpp:254
+    if (!points_xyzw || !normals_xyzw || !weights) return h->fail(DS_INVALID_ARGUMENT, "null point outputs");
+    ds_frame_outputs out{};
+    out.points_xyzw = points_xyzw;
+    out.normals_xyzw = normals_xyzw;
+    out.weights = weights;
+    out.host.rect_left = rect_left;
+    out.host.rect_right = rect_right;
+    return ds_compute_frame(h, left, right, stride, nullptr, &out);
+}
+
 DS_API int ds_find_blobs(ds_handle* h, const uint8_t* image, int width, int height, ptrdiff_t stride, ds_blob_box* out,
                          uint32_t capacity, uint32_t* found, uint32_t* kept) {
     if (!h) return DS_INVALID_ARGUMENT;

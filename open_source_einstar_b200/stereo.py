@@ -344,7 +344,7 @@ class CudaStereo:
 
     def compute_frame(self, raw_left: np.ndarray, raw_right: np.ndarray, points=None, normals=None, weights=None,
                       blobs: bool = False, on_blobs=None, rectified: bool = False) -> StereoResult:
-        """MetalStereo::compute_frame (metal_stereo.hpp:88-91), the scanner frontend's per-frame call: raw pair
+        """MetalStereo::compute_frame (metal_stereo.hpp:92-95), the scanner frontend's per-frame call: raw pair
         in; points / normals (H x W x 4 float32) and weights (H x W float32), device tensors of the caller,
         receive the frame and stay on the device; the host result holds disparity, confidence, u16 (and
         depth, the rectified pair) as compute_raw. With `blobs`, res.blobs has the marker candidates, and
@@ -380,6 +380,24 @@ class CudaStereo:
             res.blobs = (bl[:bb.kept[0]].copy(), br[:bb.kept[1]].copy())
             res.blobs_found = (int(bb.found[0]), int(bb.found[1]))
         return res
+
+    def compute_frame_raw(self, raw_left: np.ndarray, raw_right: np.ndarray, points, normals, weights,
+                          rectified: bool = False):
+        """MetalStereo::compute_frame_raw (metal_stereo.hpp:86-90): raw pair in; points / normals (H x W x 4
+        float32) and weights (H x W float32), device tensors of the caller, receive the frame and stay on the
+        device. With `rectified`, returns the rectified pair (host arrays), else None."""
+        if self.raw_size is None:
+            raise StereoError(Errc.invalid_argument, "set_rectification() not called")
+        rw, rh = self.raw_size
+        raw_left = _check_u8(raw_left, rw, rh, "raw left")
+        raw_right = _check_u8(raw_right, rw, rh, "raw right")
+        if raw_left.strides[0] != raw_right.strides[0]:
+            raw_left, raw_right = np.ascontiguousarray(raw_left), np.ascontiguousarray(raw_right)
+        rl = np.empty((self.height, self.width), np.uint8) if rectified else None
+        rr = np.empty((self.height, self.width), np.uint8) if rectified else None
+        self._check(N.lib().ds_compute_frame_raw(self._h, raw_left.ctypes.data, raw_right.ctypes.data, raw_left.strides[0],
+                                                 _ptr(points), _ptr(normals), _ptr(weights), _ptr(rl), _ptr(rr)))
+        return (rl, rr) if rectified else None
 
     def set_blob_params(self, params: "BlobParams | None" = None) -> None:
         """MetalStereo::set_blob_params (metal_stereo.cpp:279-291)."""

@@ -358,3 +358,73 @@ def _pipeline(o, left, right, p, subpixel, median, geometry, min_depth, max_dept
         f, baseline, cx_offset = geometry
         out["depth"] = o.depth(disp, f, baseline, cx_offset, min_depth, max_depth)
     return out
+
+
+def metal_blob_candidates(port: Port, img, params=None) -> np.ndarray:
+    """The reference GPU search's candidate rule as its own kernel states it: blob_select in
+    libs/depth_metal/src/stereo_kernels.metal.inc:847-901, with the ellipse orientation from
+    th = atan2(2 cxy, cxx - cyy) / 2 and cos/sin of th and of the 16 ring angles 2 pi k / 16 (numpy float32,
+    one rounding per operation), ring samples at the nearest pixel (round half away from zero, clamped).
+    Blobs and their statistics come from the restated markers::find_blobs. Returns the (k, 6) uint32 rows
+    (x0, y0, x1, y1, pixels, peak) of the blobs that pass, sorted. Pure Python per blob: small images only."""
+    import math
+    f32 = np.float32
+    img = _u8(img)
+    h, w = img.shape
+    d = dict(threshold=150, min_diameter=3, max_diameter=60, max_aspect=4.0, min_fill=0.5, border=4, max_axis_ratio=3.0,
+             ring_scale=1.4, ring_contrast=0.5, ring_max_bright=0.3)
+    if params is not None:
+        d.update({k: v for k, v in (params.items() if isinstance(params, dict) else vars(params).items()) if k in d})
+    blobs = port.find_blobs(img, int(d["threshold"]))
+    pi = f32(math.pi)
+
+    def sample(x, y):  # stereo_kernels.metal.inc:840-843
+        def rnd(v):
+            v = float(v)
+            return math.floor(v + 0.5) if v >= 0 else math.ceil(v - 0.5)
+        sx = min(max(rnd(x), 0), w - 1) if math.isfinite(float(x)) else (w - 1 if x > 0 else 0)
+        sy = min(max(rnd(y), 0), h - 1) if math.isfinite(float(y)) else (h - 1 if y > 0 else 0)
+        return f32(img[sy, sx])
+
+    out = []
+    for b in blobs:
+        x0, y0, x1, y1, px, pk, first = (int(v) for v in b[:7])
+        mo = [f32(np.int32(v)) for v in b[7:12]]
+        bw, bh = f32(x1 - x0 + 1), f32(y1 - y0 + 1)
+        if bw < f32(d["min_diameter"]) or bh < f32(d["min_diameter"]) or bw > f32(d["max_diameter"]) or bh > f32(d["max_diameter"]):
+            continue
+        if max(bw, bh) > f32(d["max_aspect"]) * min(bw, bh):
+            continue
+        if f32(px) < f32(d["min_fill"]) * bw * bh * pi / f32(4.0):
+            continue
+        m = max(3, int(max(bw, bh)) // 2)
+        bd = int(d["border"])
+        if x0 - m < bd or y0 - m < bd or x1 + m >= w - bd or y1 + m >= h - bd:
+            continue
+        n = f32(px)
+        mx, my = mo[0] / n, mo[1] / n
+        cxx, cxy, cyy = mo[2] / n - mx * mx, mo[3] / n - mx * my, mo[4] / n - my * my
+        tr = f32(0.5) * (cxx + cyy)
+        det = np.sqrt(max(f32(0.0), f32(0.25) * (cxx - cyy) * (cxx - cyy) + cxy * cxy))
+        l1, l2 = tr + det, max(tr - det, f32(0.0625))
+        ea = f32(2.0) * np.sqrt(l1) + f32(0.5)
+        eb = f32(2.0) * np.sqrt(l2) + f32(0.5)
+        if ea / eb > f32(d["max_axis_ratio"]) * f32(1.2):
+            continue
+        th = f32(0.5) * np.arctan2(f32(2.0) * cxy, cxx - cyy)
+        ct, st = np.cos(th), np.sin(th)
+        cx, cy = f32(first % w) + mx, f32(first // w) + my
+
+        def ring(scale_u, scale_v, k):
+            t = f32(2.0) * pi * f32(k) / f32(16.0)
+            u, v = scale_u * np.cos(t), scale_v * np.sin(t)
+            return sample(cx + ct * u - st * v, cy + st * u + ct * v)
+
+        bg = sorted(ring(f32(2.2) * ea, f32(2.2) * eb, k) for k in range(16))
+        level = bg[3] + f32(d["ring_contrast"]) * (f32(pk) - bg[3])
+        ru, rv = f32(d["ring_scale"]) * ea, f32(d["ring_scale"]) * eb
+        bright = sum(1 for k in range(16) if ring(ru, rv, k) > level)
+        if f32(bright) > f32(d["ring_max_bright"]) * f32(16.0):
+            continue
+        out.append((x0, y0, x1, y1, px, pk))
+    return np.array(sorted(out), np.uint32).reshape(-1, 6)

@@ -77,6 +77,48 @@ def test_candidates_include_every_sticker(port):
         assert all(tuple(int(v) for v in r) in blobs for r in boxes)
 
 
+def _sorted_rows(boxes):
+    return np.array(sorted(map(tuple, np.asarray(boxes).tolist())), np.uint32).reshape(-1, 6)
+
+
+def _rule_images():
+    imgs = [_marker_image(seed)[0] for seed in range(6)]
+    imgs += [_marker_image(9, dim=1.0)[0], _marker_image(11, dim=0.8, n=30)[0]]  # many blobs; many stickers
+    return imgs
+
+
+@pytest.mark.parametrize("params", PARAM_SETS)
+def test_candidate_rule_equals_the_reference_kernels_rule(port, params):
+    """The library's candidate rule (ellipse orientation by half-angle formulas with IEEE square roots, a
+    constant table of the 16 ring directions) selects the same blobs as the reference GPU kernel's own rule
+    (blob_select, stereo_kernels.metal.inc:847-901: atan2 / cos / sin), restated in oracle.metal_blob_candidates.
+    The library's rule is the C restatement here, which the GPU test below holds the CUDA output to."""
+    from open_source_einstar_b200 import BlobParams
+    bp = BlobParams(**params)
+    from oracle.oracle import metal_blob_candidates
+    compared = 0
+    for img in _rule_images():
+        ours, n = port.blob_candidates(img, bp, cap=1 << 16)
+        theirs = metal_blob_candidates(port, img, params)
+        assert np.array_equal(_sorted_rows(ours), theirs)
+        compared += len(theirs)
+    assert compared > 20
+
+
+@pytest.mark.gpu
+def test_cuda_candidates_equal_the_reference_kernels_rule(cuda, port):
+    """The CUDA candidates against the reference kernel's atan2 / cos / sin rule directly."""
+    from open_source_einstar_b200 import BlobParams, CudaStereo, SgmParams, StereoParams
+    from oracle.oracle import metal_blob_candidates
+    with CudaStereo.create(StereoParams(sgm=SgmParams(num_disparities=32)), 64, 48) as s:
+        for params in PARAM_SETS:
+            bp = BlobParams(**{**params, "max_blobs": 65536})
+            s.set_blob_params(bp)
+            for img in _rule_images():
+                got, found = s.find_blobs(img)
+                assert np.array_equal(_sorted_rows(got), metal_blob_candidates(port, img, params))
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("params", PARAM_SETS)
 def test_find_blobs_bit_exact(cuda, port, params):

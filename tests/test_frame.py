@@ -68,3 +68,35 @@ def test_compute_frame_errors(cuda):
         with pytest.raises(StereoError) as e:  # blobs without set_blob_params
             s.compute_frame(pr.left, pr.right, blobs=True)
         assert e.value.code == Errc.invalid_argument
+
+
+def test_compute_frame_raw_equals_compute_frame(cuda):
+    """ds_compute_frame_raw (MetalStereo::compute_frame_raw): the same points, normals and weights as
+    compute_frame, the rectified pair as compute_raw returns it, and the reference's errors."""
+    import torch
+    from open_source_einstar_b200 import (CudaStereo, Errc, RectifiedGeometry, RemapTable, SgmParams, StereoError,
+                                          StereoParams, synth)
+    pr = synth.raw_objects_pair(seed=12, width=640, height=512, f=560.0, num_disparities=64, n_objects=8, device="cuda")
+    (lx, ly), (rx, ry) = pr.maps
+    w, h = 320, 256
+    sp = StereoParams(sgm=SgmParams(min_disparity=pr.min_disparity // 4 - 2, num_disparities=40), pyramid_levels=1,
+                      median=False, detail_enabled=True, filter_occlusion=True, filter_spikes=True,
+                      speckle_max_region_size=100)
+    geom = RectifiedGeometry(pr.f / 2, (w - 1) / 2.0, (h - 1) / 2.0, pr.baseline, 0.0)
+    bufs = lambda: (torch.zeros((h, w, 4), dtype=torch.float32, device=cuda),
+                    torch.zeros((h, w, 4), dtype=torch.float32, device=cuda), torch.zeros((h, w), dtype=torch.float32, device=cuda))
+    with CudaStereo.create(sp, w, h) as s:
+        s.set_rectification(RemapTable(lx, ly), RemapTable(rx, ry), 640, 512)
+        p0, n0, w0 = bufs()
+        with pytest.raises(StereoError) as e:  # metal_stereo.cpp:254
+            s.compute_frame_raw(pr.left, pr.right, p0, n0, w0)
+        assert e.value.code == Errc.invalid_argument and "set_point_params" in e.value.message
+        s.set_point_params(geom, 150.0, 700.0, 4.0)
+        want = s.compute_frame(pr.left, pr.right, p0, n0, w0, rectified=True)
+        p1, n1, w1 = bufs()
+        rl, rr = s.compute_frame_raw(pr.left, pr.right, p1, n1, w1, rectified=True)
+        torch.cuda.synchronize()
+        assert np.array_equal(rl, want.rect_left) and np.array_equal(rr, want.rect_right)
+        for a, b in ((p0, p1), (n0, n1), (w0, w1)):
+            assert torch.equal(a.view(torch.int32), b.view(torch.int32))
+        assert s.compute_frame_raw(pr.left, pr.right, p1, n1, w1) is None

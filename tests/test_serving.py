@@ -151,3 +151,41 @@ def test_server_rejects_bad_requests(cuda):
             srv.submit(pr.left, pr.right, w, h, bad, out, calib=0)
         assert e.value.code == Errc.invalid_argument
         assert srv.stats()["submitted"] == 0
+
+
+def test_server_config4_sizes_against_the_reference(cuda, ref, port):
+    """Frames of configuration 4's three sizes (1280x1024 D=128, 960x768 D=96, 640x512 D=96; raw pairs, GPU
+    remap) queued together on the server: each result equals the reference pipeline directly (the restated
+    remap, the reference's sgm_disparity + median3, the restated depth), not only a per-frame CUDA run."""
+    from open_source_einstar_b200 import SgmParams, StereoParams, synth
+    from oracle.oracle import OracleSgm
+    specs = [(1280, 1024, 128), (960, 768, 96), (640, 512, 96)]
+    rigs = []
+    for i, (w, h, d) in enumerate(specs):
+        pr = synth.raw_objects_pair(seed=300 + i, width=w, height=h, f=1100.0 * w / 1280, num_disparities=d,
+                                    device="cuda")
+        rigs.append((w, h, d, pr))
+    with _server(rigs, max_slots=3) as srv:
+        frames = _frames(rigs, 6, seed=7)
+        for c in range(len(rigs)):  # every size at least once
+            frames[c] = _frames([rigs[c]], 1, seed=c)[0]
+            frames[c]["calib"] = c
+        tickets = [srv.submit(f["left"], f["right"], f["width"], f["height"], f["params"], f["outputs"], f["calib"],
+                              tag=i) for i, f in enumerate(frames)]
+        done = srv.wait_all(tickets)
+    want = {}
+    for c, (w, h, d, pr) in enumerate(rigs):
+        (lx, ly), (rx, ry) = pr.maps
+        p = OracleSgm(min_disparity=pr.min_disparity, num_disparities=d)
+        rl, rr = port.remap(pr.left, lx, ly), port.remap(pr.right, rx, ry)
+        disp = ref.median3(ref.sgm_disparity(rl, rr, p))
+        want[c] = (disp, port.encode_u16(disp, p.min_disparity),
+                   port.depth(disp, pr.f, pr.baseline, pr.cx_offset, 150.0, 700.0))
+    for i, (f, t) in enumerate(zip(frames, tickets)):
+        assert done[t].ok, f"frame {i}: status {done[t].status}"
+        disp, u16, z = want[f["calib"]]
+        o = f["outputs"]
+        assert same_bits(o["disparity"], disp), f"frame {i} ({f['width']}x{f['height']}): {mismatch_report(o['disparity'], disp)}"
+        assert np.array_equal(o["disparity_u16"], u16)
+        nz = z > 0
+        assert np.all(np.abs(o["depth"][nz] - z[nz]) <= DEPTH_RTOL * z[nz]) and same_bits(o["depth"], z)

@@ -41,7 +41,10 @@ def test_noalloc_matches_allocating_entry_point(cuda, golden):
     from open_source_einstar_b200 import SgmParams, StereoParams
     from open_source_einstar_b200._native import lib
     L = lib()
-    cases = ["plane_sphere_160x128", "census_7x7_u64", "eight_paths", "d_not_multiple_of_32_d40"]
+    # u8 and u16 path values (census_9x7_wide), 64-bit census words, 8 paths, D not a multiple of the lane
+    # slab, a negative minimum disparity, and D=5 where most lanes are padding
+    cases = ["plane_sphere_160x128", "census_7x7_u64", "eight_paths", "d_not_multiple_of_32_d40", "census_9x7_wide",
+             "negative_min_disparity", "tiny_37x29_d5"]
     for name in cases:
         c = golden[name]
         p = OracleSgm(**c["params"])
@@ -72,3 +75,39 @@ def test_noalloc_rejects_requests_beyond_its_scratch(cuda):
     assert rc == 5  # DS_INVALID_ARGUMENT
     msg = L.ds_last_global_error().decode()
     assert "scratch" in msg and "bytes" in msg
+
+
+SCRATCH_BYTES = 16 << 20  # the documented limit of the static array
+
+
+def _scratch_need(w, h, nd, census_window=25, paths=4, wide=False):
+    """The bytes the entry point needs (its documented sizing): two census images of 4-byte words (8 for
+    windows of more than 32 neighbours) and the path values of all directions with the lane slabs of the
+    library's default shape for nd, each part rounded up to 256 bytes."""
+    a256 = lambda v: (v + 255) // 256 * 256
+    dp = next(seg * 2 * r for lim, r, seg in ((32, 1, 16), (64, 2, 16), (96, 3, 16), (128, 4, 16), (192, 3, 32),
+                                              (256, 4, 32), (384, 6, 32), (512, 8, 32)) if nd <= lim)
+    cw = 8 if census_window - 1 > 32 else 4
+    return 2 * a256(w * h * cw) + a256(w * h * dp * paths * (2 if wide else 1))
+
+
+def test_noalloc_limit_boundary(cuda):
+    """The documented example (320 x 240 at 32 disparities, 4 paths) fits; at 320 columns and 32 disparities
+    the tallest image that fits is accepted and one row more is refused with the bytes it would need."""
+    import torch
+    from open_source_einstar_b200 import SgmParams, StereoParams
+    from open_source_einstar_b200._native import lib
+    L = lib()
+    sgm_c = StereoParams(sgm=SgmParams(num_disparities=32)).c().sgm
+    assert _scratch_need(320, 240, 32) <= SCRATCH_BYTES
+    h_max = max(h for h in range(1, 2000) if _scratch_need(320, h, 32) <= SCRATCH_BYTES)
+    for h, ok in ((240, True), (h_max, True), (h_max + 1, False)):
+        img = torch.zeros((h, 320), dtype=torch.uint8, device="cuda")
+        out = torch.zeros((h, 320), dtype=torch.float32, device="cuda")
+        rc = _noalloc(L, sgm_c, img, img, out)
+        torch.cuda.synchronize()
+        if ok:
+            assert rc == 0, (h, L.ds_last_global_error().decode())
+        else:
+            assert rc == 5, h
+            assert str(_scratch_need(320, h, 32)) in L.ds_last_global_error().decode()
