@@ -22,7 +22,7 @@ NVCC_FLAGS = [
     "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared", "-cudart", "static",
 ]
 
-SOURCES = ["depth_cuda.cu", "noalloc.cu", "server.cu", "points.cu", "recording.cu", "sweep_cols.cu", "sweep_rows.cu", "inst_r1.cu", "inst_r2.cu", "inst_r3.cu", "inst_r4.cu", "inst_r6.cu", "inst_r8.cu"]
+SOURCES = ["depth_cuda.cu", "noalloc.cu", "server.cu", "points.cu", "recording.cu", "sweep_cols.cu", "sweep_rows.cu", "wta.cu", "inst_r1.cu", "inst_r2.cu", "inst_r3.cu", "inst_r4.cu", "inst_r6.cu", "inst_r8.cu"]
 
 
 def _nvcc() -> str:

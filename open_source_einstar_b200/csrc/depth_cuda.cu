@@ -17,6 +17,7 @@
 #include "dispatch.h"
 #include "frame_kernels.cuh"
 #include "sweep_kernels.cuh"
+#include "wta_kernels.cuh"
 #include "internal.h"
 #include "refine_kernels.cuh"
 #include "blob_kernels.cuh"
@@ -358,9 +359,40 @@ void launch_paths(ds_handle* h, cudaStream_t st) {
     ++g_launches;
 }
 
+// Whether the WTA of the per-direction path runs as row sweeps (wta_kernels.cuh): 4 paths with byte path
+// values whose pairs fit a byte, and lane slabs of 48, 64, 96 or 128 disparities.
+bool wta_rows_fit(const ds_handle* h) {
+    int chunk = 0, lg = 0, sets = 0;
+    return !h->cfg.fused && h->ndirs == 4 && !h->wide && !h->s16 && ds::wta_rows_layout(h->w, h->dp, chunk, lg, sets);
+}
+
+dsk::WtaRowArgs wta_row_args(const ds_handle* h) {
+    dsk::WtaRowArgs a{};
+    a.values = static_cast<const uint8_t*>(h->d_values);
+    a.dir_stride = h->dir_stride;
+    a.rec = h->d_rec;
+    a.rk = h->d_rk;
+    a.disp = h->d_disp_lr;
+    a.w = h->w;
+    a.h = h->h;
+    a.nd = h->nd;
+    a.dp = h->dp;
+    a.min_disp = h->p.sgm.min_disparity;
+    a.uniqueness = h->p.sgm.uniqueness;
+    a.subpixel = h->p.subpixel ? 1 : 0;
+    a.lr_max_diff = h->p.sgm.lr_max_diff;
+    ds::wta_rows_layout(h->w, h->dp, a.chunk, a.lg_chunks, a.sets);
+    return a;
+}
+
 void launch_wta(ds_handle* h, cudaStream_t st) {
     if (h->cfg.fused) {
         DS_CUDA(ds::launch_sweep_rows(h->cfg, sweep_slant(h), sweep_pad(h), sweep_args(h), st));
+        ++g_launches;
+        return;
+    }
+    if (wta_rows_fit(h)) {
+        DS_CUDA(ds::launch_wta_rows(wta_row_args(h), st));
         ++g_launches;
         return;
     }
@@ -390,30 +422,42 @@ void free_counted(ds_handle* h, void*& p, size_t bytes) {
     }
 }
 
+// WTA records (8 bytes per pixel) and right-WTA keys (2 bytes per pixel and key set: 2 sets for the sweep
+// kernels, up to kWtaRowMaxSets for the row-sweep WTA), after the path values in the volume.
+size_t aux_bytes(const ds_handle* h) {
+    const size_t n = static_cast<size_t>(h->w) * h->h;
+    return (n * 8 + 255) / 256 * 256 + n * 2 * (h->cfg.fused ? 2 : dsk::kWtaRowMaxSets);
+}
 // The sweep kernels' buffers inside the path-value volume: S, T and C slabs (u8 [y][x][dp] with kGuardRows
-// guard rows above and below), then the WTA records (8 bytes per pixel) and the right-WTA keys (2 x 2 bytes).
+// guard rows above and below), then the WTA records and the right-WTA keys.
 size_t sweep_slab_bytes(const ds_handle* h) {
     return (static_cast<size_t>(h->h + 2 * dsk::kGuardRows) * h->w * h->dp + 255) / 256 * 256;
 }
-size_t sweep_volume_bytes(const ds_handle* h) {
-    const size_t n = static_cast<size_t>(h->w) * h->h;
-    return 3 * sweep_slab_bytes(h) + (n * 8 + 255) / 256 * 256 + n * 4;
+size_t sweep_volume_bytes(const ds_handle* h) { return 3 * sweep_slab_bytes(h) + aux_bytes(h); }
+size_t direction_slab_bytes(const ds_handle* h) {  // the per-direction path's values
+    return (h->dir_stride * h->ndirs * (h->wide ? 2 : 1) + 255) / 256 * 256;
 }
 void bind_sweep_buffers(ds_handle* h) {
-    if (!h->cfg.fused || !h->d_values) {
-        h->d_S = h->d_T = h->d_C = nullptr;
-        h->d_rec = nullptr;
-        h->d_rk = nullptr;
+    h->d_S = h->d_T = h->d_C = nullptr;
+    h->d_rec = nullptr;
+    h->d_rk = nullptr;
+    if (!h->d_values) return;
+    const size_t n = static_cast<size_t>(h->w) * h->h;
+    uint8_t* base = static_cast<uint8_t*>(h->d_values);
+    size_t at = 0;
+    if (h->cfg.fused) {
+        const size_t slab = sweep_slab_bytes(h), lead = static_cast<size_t>(dsk::kGuardRows) * h->w * h->dp;
+        h->d_S = base + lead;
+        h->d_T = base + slab + lead;
+        h->d_C = base + 2 * slab + lead;
+        at = 3 * slab;
+    } else if (wta_rows_fit(h)) {
+        at = direction_slab_bytes(h);
+    } else {
         return;
     }
-    const size_t n = static_cast<size_t>(h->w) * h->h;
-    const size_t slab = sweep_slab_bytes(h), lead = static_cast<size_t>(dsk::kGuardRows) * h->w * h->dp;
-    uint8_t* base = static_cast<uint8_t*>(h->d_values);
-    h->d_S = base + lead;
-    h->d_T = base + slab + lead;
-    h->d_C = base + 2 * slab + lead;
-    h->d_rec = reinterpret_cast<uint2*>(base + 3 * slab);
-    h->d_rk = reinterpret_cast<uint16_t*>(base + 3 * slab + (n * 8 + 255) / 256 * 256);
+    h->d_rec = reinterpret_cast<uint2*>(base + at);
+    h->d_rk = reinterpret_cast<uint16_t*>(base + at + (n * 8 + 255) / 256 * 256);
 }
 
 constexpr int kCensusSlack = 40;
@@ -450,7 +494,8 @@ void size_config_buffers(ds_handle* h) {
         for (int s = 0; s < 2; ++s)
             h->d_census[s] = static_cast<uint8_t*>(h->census_raw[s]) + (static_cast<size_t>(g) * pitch + guard) * cw;
     }
-    const size_t vb = h->cfg.fused ? sweep_volume_bytes(h) : h->dir_stride * h->ndirs * (h->wide ? 2 : 1);
+    const size_t vb = h->cfg.fused ? sweep_volume_bytes(h)
+                                   : direction_slab_bytes(h) + (wta_rows_fit(h) ? aux_bytes(h) : 0);
     const size_t cb = h->cfg.materialize && !h->cfg.fused ? n * static_cast<size_t>(h->dp) : 0;
     if (h->external_volumes) {  // a batch or the request server binds shared volumes later
         h->values_bytes = vb;
@@ -1632,6 +1677,8 @@ struct BatchGroup {
     ds::KernelCfg cfg;
     bool c64 = false, wide = false;
     int ndirs = 4;
+    int dp = 0;        // row-sweep WTA groups: lane slab and padding
+    bool pad = false;
     size_t smem = 0;
     std::vector<int> pairs, prefix, gx, gy;
     int total = 0;
@@ -1673,19 +1720,22 @@ struct ds_batch {
     std::vector<dsk::WtaArgs> a_wta;
     std::vector<dsk::PostArgs> a_post;
     std::vector<dsk::SweepArgs> a_sweep;  // by value into the graph: they name only the pair's own buffers
+    std::vector<dsk::WtaRowArgs> a_wrow;
     dsk::RectifyArgs* d_rect = nullptr;
     dsk::CensusArgs* d_census = nullptr;
     dsk::CostArgs* d_costs = nullptr;
     dsk::PathArgs* d_paths = nullptr;
     dsk::WtaArgs* d_wta = nullptr;
     dsk::PostArgs* d_post = nullptr;
+    dsk::WtaRowArgs* d_wrow = nullptr;
     struct Micro {
         std::vector<int> pairs;  // heaviest first
         BatchGroup g_rect, g_post;
-        std::vector<BatchGroup> g_census, g_costs, g_paths, g_wta;
+        std::vector<BatchGroup> g_census, g_costs, g_paths, g_wta, g_wrow;
         std::vector<int> sweep;  // pairs on the sweep kernels: one column and one row launch each
         int launches() const {
-            return (g_rect.total > 0 ? 1 : 0) + static_cast<int>(g_census.size() + g_costs.size() + g_paths.size() + g_wta.size()) +
+            return (g_rect.total > 0 ? 1 : 0) +
+                   static_cast<int>(g_census.size() + g_costs.size() + g_paths.size() + g_wta.size() + g_wrow.size()) +
                    2 * static_cast<int>(sweep.size()) + 1;
         }
     };
@@ -1731,12 +1781,13 @@ void batch_release(ds_batch* b) {
         for (auto* p : c.map)
             if (p) cudaFree(p);
     for (void* p : {static_cast<void*>(b->d_rect), static_cast<void*>(b->d_census), static_cast<void*>(b->d_costs),
-                    static_cast<void*>(b->d_paths), static_cast<void*>(b->d_wta), static_cast<void*>(b->d_post)})
+                    static_cast<void*>(b->d_paths), static_cast<void*>(b->d_wta), static_cast<void*>(b->d_post),
+                    static_cast<void*>(b->d_wrow)})
         if (p) cudaFree(p);
     for (auto& m : b->micro) {
         m.g_rect.release();
         m.g_post.release();
-        for (auto* gs : {&m.g_census, &m.g_costs, &m.g_paths, &m.g_wta})
+        for (auto* gs : {&m.g_census, &m.g_costs, &m.g_paths, &m.g_wta, &m.g_wrow})
             for (auto& g : *gs) g.release();
     }
     for (auto s : b->branch_st)
@@ -1756,6 +1807,7 @@ void batch_fill_args(ds_batch* b) {
     b->a_wta.assign(n, {});
     b->a_post.assign(n, {});
     b->a_sweep.assign(n, {});
+    b->a_wrow.assign(n, {});
     for (int i = 0; i < n; ++i) {
         ds_handle* h = b->h[i];
         const ds_pair_desc& d = b->desc[i];
@@ -1831,6 +1883,7 @@ void batch_fill_args(ds_batch* b) {
         wa.lr_max_diff = sg.lr_max_diff;
         wa.disp = h->d_disp_lr;
         wa.pair_sums = h->s16 ? 0 : 1;
+        if (wta_rows_fit(h)) b->a_wrow[i] = wta_row_args(h);
         auto& q = b->a_post[i];
         const ds_outputs& o = b->out[i];
         q.disp = h->d_disp_lr;
@@ -1859,6 +1912,7 @@ void batch_fill_args(ds_batch* b) {
     put(b->a_paths, b->d_paths);
     put(b->a_wta, b->d_wta);
     put(b->a_post, b->d_post);
+    put(b->a_wrow, b->d_wrow);
     b->args_dirty = false;
 }
 
@@ -1970,7 +2024,17 @@ void batch_plan_micro(ds_batch* b, ds_batch::Micro& m, const std::vector<int>& o
             const int gx = (max_lines + lpb - 1) / lpb;
             add(g, i, gx * h->ndirs, gx, 1);
         }
-        {
+        if (wta_rows_fit(h)) {
+            const bool pad = h->nd < h->dp;
+            BatchGroup& g = find_or_add(m.g_wrow, [&](const BatchGroup& x) { return x.dp == h->dp && x.pad == pad; });
+            g.dp = h->dp;
+            g.pad = pad;
+            int R = 0, seg = 0, chunk = 0, lg = 0, sets = 0;
+            ds::wta_rows_shape(h->dp, R, seg);
+            ds::wta_rows_layout(h->w, h->dp, chunk, lg, sets);
+            const int rows = (dsk::kWtaRowWarps * 32 / seg) >> lg;
+            add(g, i, (h->h + rows - 1) / rows, 1, 1);
+        } else {
             BatchGroup& g = find_or_add(m.g_wta, [&](const BatchGroup& x) {
                 return x.cfg.R == c.R && x.cfg.seg == c.seg && x.cfg.wta_threads == c.wta_threads && x.wide == h->wide &&
                        x.ndirs == h->ndirs;
@@ -1984,7 +2048,7 @@ void batch_plan_micro(ds_batch* b, ds_batch::Micro& m, const std::vector<int>& o
     }
     m.g_rect.upload();
     m.g_post.upload();
-    for (auto* gs : {&m.g_census, &m.g_costs, &m.g_paths, &m.g_wta})
+    for (auto* gs : {&m.g_census, &m.g_costs, &m.g_paths, &m.g_wta, &m.g_wrow})
         for (auto& g : *gs) g.upload();
 }
 
@@ -2043,6 +2107,10 @@ void batch_enqueue_micro(ds_batch* b, const ds_batch::Micro& m, cudaStream_t st,
     }
     for (const auto& g : m.g_wta) {
         DS_CUDA(ds::launch_wta_batch(g.cfg, g.wide, g.ndirs, b->d_wta, g.dev(), g.smem, st));
+        ++g_launches;
+    }
+    for (const auto& g : m.g_wrow) {
+        DS_CUDA(ds::launch_wta_rows_batch(g.dp, g.pad, b->d_wrow, g.dev(), st));
         ++g_launches;
     }
     mark(5);

@@ -14,6 +14,7 @@ struct PathArgs;
 struct WtaArgs;
 struct CostArgs;
 struct SweepArgs;
+struct WtaRowArgs;
 }  // namespace dsk
 
 namespace ds {
@@ -48,7 +49,14 @@ cudaError_t launch_costs(const KernelCfg& cfg, bool c64, const dsk::CostArgs& a,
 cudaError_t launch_sweep_cols(const KernelCfg& cfg, bool slant, bool pad, const dsk::SweepArgs& a, cudaStream_t st);
 cudaError_t launch_sweep_rows(const KernelCfg& cfg, bool slant, bool pad, const dsk::SweepArgs& a, cudaStream_t st);
 
+// Row-sweep WTA of the per-direction path (wta_kernels.cuh): lane slab shapes, the chunks of a row of width w
+// (columns per chunk, log2 of the chunk count, key sets), and the launches.
+bool wta_rows_shape(int dp, int& R, int& seg);
+bool wta_rows_layout(int w, int dp, int& chunk, int& lg_chunks, int& sets);
+cudaError_t launch_wta_rows(const dsk::WtaRowArgs& a, cudaStream_t st);
+
 struct BatchGroupDev;
+cudaError_t launch_wta_rows_batch(int dp, bool pad, const dsk::WtaRowArgs* args, const BatchGroupDev& g, cudaStream_t st);
 
 // Persistent batch launches (one launch walks the blocks of every pair of a kernel-variant group).
 cudaError_t launch_paths_batch(const KernelCfg& cfg, bool c64, bool wide, const dsk::PathArgs* args, const BatchGroupDev& g,
