@@ -229,7 +229,7 @@ typedef struct ds_batch ds_batch;
 
 /* Scheduling of a batch: pairs (heaviest first) are cut into micro-batches of `micro_batch` pairs that go
  * through all stages back to back (so a pair's volumes are consumed while still in L2), and the
- * micro-batches run round-robin on `branches` parallel branches of the graph. 0 = defaults (1, 4).
+ * micro-batches run round-robin on `branches` parallel branches of the graph. 0 = defaults (1, 8).
  * Micro-batches on one branch run one after another, so they share cost and path-value volumes: the
  * batch holds branches x micro_batch volumes (each sized for the largest pair it serves), not one per
  * pair. */

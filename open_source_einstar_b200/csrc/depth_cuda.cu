@@ -1742,7 +1742,7 @@ struct ds_batch {
     std::vector<Micro> micro;  // pairs in micro-batches run through all stages back to back
     std::vector<void*> volumes;  // shared cost / path-value volumes, one per (branch, position) slot
     size_t volume_bytes = 0;
-    int micro_batch = 1, branches = 4;  // best measured for 1280x1024, D=128 on B200
+    int micro_batch = 1, branches = 8;  // best measured for 16 pairs of 1280x1024, D=128 on B200
     std::vector<cudaStream_t> branch_st;
     std::vector<cudaEvent_t> fork_join;
     cudaStream_t stream = nullptr;

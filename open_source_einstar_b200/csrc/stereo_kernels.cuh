@@ -151,13 +151,46 @@ __device__ __forceinline__ void cost_tile_body(const CostArgs& a, int b, CW* sm)
     }
     for (int i = threadIdx.x; i < nx; i += blockDim.x) sl[i] = __ldg(cl + x0 + i);
     __syncthreads();
+    const uint32_t inv = static_cast<uint32_t>(a.invalid_cost);
+    // Interior tiles: every right column of the window inside the row, no per-cost range test.
+    const bool interior = r0 >= 0 && r0 + nr <= a.w;
+    if constexpr (NC == 4) {
+        if ((a.dp & 15) == 0) {
+            // Sixteen costs a thread: thread t of a pixel takes the cost words t + j * tq (j < 4, tq = dp / 16
+            // threads per pixel), so the threads of a pixel read consecutive 16-byte chunks of one shifted copy
+            // and store consecutive words; four popcounts are packed by multiply-adds (FMA pipe).
+            const int tq = a.dp >> 4;
+            const int ppp = static_cast<int>(blockDim.x) / tq;
+            const int t = threadIdx.x % tq, pi = threadIdx.x / tq;
+            if (pi >= ppp) return;
+            for (int px = pi; px < nx; px += ppp) {
+                const CW vl = sl[px];
+                uint32_t* dst = reinterpret_cast<uint32_t*>(a.costs + (static_cast<size_t>(y) * a.w + x0 + px) * a.dp);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int w = t + j * tq;
+                    const int g = px + a.dp - 4 - 4 * w;  // window slot of disparity 4w + 3
+                    const int c = g & 3;
+                    const uint4 q = *reinterpret_cast<const uint4*>(sm + c * cpy + g - c);
+                    uint32_t b0 = popcount_word<CW>(vl ^ q.w), b1 = popcount_word<CW>(vl ^ q.z);
+                    uint32_t b2 = popcount_word<CW>(vl ^ q.y), b3 = popcount_word<CW>(vl ^ q.x);
+                    if (!interior) {  // byte jj: right column r0 + g + 3 - jj
+                        const int xr = r0 + g + 3;
+                        b0 = static_cast<unsigned>(xr) < static_cast<unsigned>(a.w) ? b0 : inv;
+                        b1 = static_cast<unsigned>(xr - 1) < static_cast<unsigned>(a.w) ? b1 : inv;
+                        b2 = static_cast<unsigned>(xr - 2) < static_cast<unsigned>(a.w) ? b2 : inv;
+                        b3 = static_cast<unsigned>(xr - 3) < static_cast<unsigned>(a.w) ? b3 : inv;
+                    }
+                    dst[w] = (b3 * 256u + b2) * 65536u + (b1 * 256u + b0);
+                }
+            }
+            return;
+        }
+    }
     const int tp = a.dp >> 2;  // threads per pixel
     const int ppp = static_cast<int>(blockDim.x) / tp;
     const int t = threadIdx.x % tp, pi = threadIdx.x / tp;
     if (pi >= ppp) return;
-    const uint32_t inv = static_cast<uint32_t>(a.invalid_cost);
-    // Interior tiles: every right column of the window inside the row, no per-cost range test.
-    const bool interior = r0 >= 0 && r0 + nr <= a.w;
     for (int px = pi; px < nx; px += ppp) {
         const CW vl = sl[px];
         const int g = px + a.dp - 4 - 4 * t;  // window slot of disparity 4t + 3; slot g + 3 - j is disparity 4t + j
