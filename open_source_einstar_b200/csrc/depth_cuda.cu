@@ -1018,6 +1018,9 @@ cudaError_t launch_costs_batch(const KernelCfg& cfg, bool c64, const dsk::CostAr
 namespace dsk {
 
 // Persistent batch launches of the per-pixel stages; per group pair i: grid gx[i] x gy[i] x (2 or 1).
+// Virtual blocks of the 2D stages cover a run of tiles along x (one decode and argument check per run).
+constexpr int kRectifyRun = 2, kTileRun = 4;
+
 __device__ __forceinline__ void decode3(int lb, int gx, int gy, int& bx, int& by, int& bz) {
     bx = lb % gx;
     const int t = lb / gx;
@@ -1045,7 +1048,8 @@ __global__ void kb_rectify(const RectifyArgs* __restrict__ args, const int* __re
         int bx, by, bz;
         decode3(v - __ldg(prefix + i), __ldg(gx + i), __ldg(gy + i), bx, by, bz);
         stage_args(sa, args, __ldg(pairs + i), cur);
-        rectify_body(sa, bx, by, bz);
+#pragma unroll 1
+        for (int j = 0; j < kRectifyRun; ++j) rectify_body(sa, bx * kRectifyRun + j, by, bz);
     }
 }
 
@@ -1059,7 +1063,8 @@ __global__ void kb_census(const CensusArgs* __restrict__ args, const int* __rest
         int bx, by, bz;
         decode3(v - __ldg(prefix + i), __ldg(gx + i), __ldg(gy + i), bx, by, bz);
         stage_args(sa, args, __ldg(pairs + i), cur);
-        census_body<W>(sa, bx, by, bz);
+#pragma unroll 1
+        for (int j = 0; j < kTileRun; ++j) census_body<W>(sa, bx * kTileRun + j, by, bz);
     }
 }
 
@@ -1086,7 +1091,8 @@ __global__ void kb_post(const PostArgs* __restrict__ args, const int* __restrict
         int bx, by, bz;
         decode3(v - __ldg(prefix + i), __ldg(gx + i), __ldg(gy + i), bx, by, bz);
         stage_args(sa, args, __ldg(pairs + i), cur);
-        post_body(sa, bx, by);
+#pragma unroll 1
+        for (int j = 0; j < kTileRun; ++j) post_body(sa, bx * kTileRun + j, by);
     }
 }
 
@@ -1991,12 +1997,13 @@ void batch_plan_micro(ds_batch* b, ds_batch::Micro& m, const std::vector<int>& o
         ds_handle* h = b->h[i];
         const int tx = (h->w + 31) / 32, ty = (h->h + 7) / 8;
         const int tx4 = (h->w + 32 * dsk::kRectifyPixelsPerThread - 1) / (32 * dsk::kRectifyPixelsPerThread);
-        if (b->desc[i].raw) add(m.g_rect, i, tx4 * ty * 2, tx4, ty);
-        add(m.g_post, i, tx * ty, tx, ty);
+        const int rx4 = (tx4 + dsk::kRectifyRun - 1) / dsk::kRectifyRun, rx = (tx + dsk::kTileRun - 1) / dsk::kTileRun;
+        if (b->desc[i].raw) add(m.g_rect, i, rx4 * ty * 2, rx4, ty);
+        add(m.g_post, i, rx * ty, rx, ty);
         {
             BatchGroup& g = find_or_add(m.g_census, [&](const BatchGroup& x) { return x.c64 == h->census64; });
             g.c64 = h->census64;
-            add(g, i, tx * ty * 2, tx, ty);
+            add(g, i, rx * ty * 2, rx, ty);
         }
         const ds::KernelCfg& c = h->cfg;
         if (c.fused) {

@@ -109,12 +109,14 @@ __device__ __forceinline__ void census_body(const CensusArgs& a, int bx, int by,
     const int x0 = bx * 32, y0 = by * 8;
     const uint8_t* img = bz ? a.img[1] : a.img[0];  // selected, not indexed (see rectify_body)
     const int tw = 32 + 2 * a.rx, th = 8 + 2 * a.ry;
-    const int tid = threadIdx.y * 32 + threadIdx.x;
     __syncthreads();  // the previous virtual block's readers are done
-    for (int i = tid; i < tw * th; i += 256) {
-        const int ty = i / tw, tx = i - ty * tw;
-        const int gx = x0 - a.rx + tx, gy = y0 - a.ry + ty;
-        tile[ty][tx] = (gx >= 0 && gx < a.w && gy >= 0 && gy < a.h) ? __ldg(img + static_cast<size_t>(gy) * a.w + gx) : 0;
+    for (int ty = threadIdx.y; ty < th; ty += 8) {  // block (32, 8)
+        const int gy = y0 - a.ry + ty;
+        const bool row_in = gy >= 0 && gy < a.h;
+        for (int tx = threadIdx.x; tx < tw; tx += 32) {
+            const int gx = x0 - a.rx + tx;
+            tile[ty][tx] = (row_in && gx >= 0 && gx < a.w) ? __ldg(img + static_cast<size_t>(gy) * a.w + gx) : 0;
+        }
     }
     __syncthreads();
     const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
