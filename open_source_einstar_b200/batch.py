@@ -71,6 +71,7 @@ class StereoBatch:
             raise StereoError(rc, L.ds_last_global_error().decode())
         self._b = h
         self.pairs = list(pairs)
+        self._bound: dict = {}
 
     def _check(self, rc):
         if rc != 0:
@@ -80,6 +81,7 @@ class StereoBatch:
         if self._b:
             N.lib().ds_batch_destroy(self._b)
             self._b = C.c_void_p()
+        self._bound = {}
 
     def __del__(self):
         try:
@@ -99,11 +101,14 @@ class StereoBatch:
                                                        left.height, int(raw_width), int(raw_height)))
 
     def bind(self, i: int, left, right, outputs: dict | None = None):
-        """Device buffers of pair i (inputs tightly packed; outputs keyed like ds_outputs)."""
+        """Device buffers of pair i (inputs tightly packed; outputs keyed like ds_outputs). The batch keeps a
+        reference to every bound tensor until it is re-bound or the batch closes: the graph holds their device
+        addresses, and a tensor freed by its caller would hand its memory to the next allocation."""
         outputs = outputs or {}
         o = N.OutputsC(*[_ptr(outputs.get(k)) for k in ("disparity", "confidence", "disparity_u16", "depth",
                                                         "rect_left", "rect_right")])
         self._check(N.lib().ds_batch_bind(self._b, int(i), _ptr(left), _ptr(right), C.byref(o)))
+        self._bound[int(i)] = (left, right, dict(outputs))
 
     def run(self, stream=None, graph: bool = True):
         fn = N.lib().ds_batch_run if graph else N.lib().ds_batch_run_eager
