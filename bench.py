@@ -13,9 +13,15 @@ Printed as one JSON line by rank 0:
   e2e            the same through the public host API (OfflineRedepth over StereoBatch): host->device copy of
                  every step's raw pairs and device->host copy of their u16 disparity + f32 depth inside the
                  timed region (double-buffered across steps), device-timed
+  e2e_plugin     the drop-in call (ds_compute_raw), one frame per synchronous call from pinned host memory to
+                 pinned host memory, host-clock latency p50 / p99
   frame_ms       per-frame device time percentiles (stage events)
   roofline       the dominant kernel (SGM paths) against the measured HBM copy bandwidth
   cpu_baseline   the reference CPU path (oracle/_ref: the reference's stereo.cpp) on this host's cores
+  serving, batch64, offline
+                 on one GPU (unless --no-extras): configuration 4 (request server, Poisson arrivals, latency
+                 percentiles), configuration 3 (64 uneven pairs, batched against per-frame launches) and
+                 configuration 5 (offline 8-path D=256 re-depth of a 64-frame synthetic recording)
 With --impl reference, the reference CPU implementation alone is timed (rank 0 only).
 Multi-GPU: independent replicas (frames shard across ranks, no collective on the data path).
 """
@@ -425,19 +431,26 @@ def batch64_line(dev, steps, warmup, world=1, rank=0, tune_schedule=True):
 
 # ---- offline re-depth: a raw recording in batches of 128 at D=256, 8 paths, u16 path values -----------------
 def run_offline(args, world, rank, local):
-    """A synthetic handheld recording (150 mm object, 250-450 mm standoff, raw 1280x1024 IR pairs) re-depthed
-    in batches of --offline-batch frames: 8-path SGM, D=256, 16-bit path values. Frames are rendered into
-    pinned host memory first (untimed); the timed run covers host->device copies, the batched graph
-    replays and device->host copies of u16 disparity and depth, double-buffered."""
+    """Configuration 5 on its own line (see offline_line)."""
     import torch
+    torch.cuda.set_device(local)
+    line = offline_line(torch.device("cuda", local), args.recording_frames, args.offline_batch, world, rank, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def offline_line(dev, n, batch, world=1, rank=0, local=0):
+    """A synthetic handheld recording (150 mm object, 250-450 mm standoff, raw 1280x1024 IR pairs) of `n`
+    frames re-depthed in batches of `batch` frames: 8-path SGM, D=256, 16-bit path values. Frames are
+    rendered into pinned host memory first (untimed); the timed run covers host->device copies, the batched
+    graph replays and device->host copies of u16 disparity and depth, double-buffered. Three frames are
+    checked against the per-frame path first. Returns the JSON line (configuration 5)."""
     from open_source_einstar_b200 import CudaStereo, RectifiedGeometry, RemapTable, SgmParams, StereoParams, synth
     from open_source_einstar_b200.autotune import Autotuner, FrameKind
     from open_source_einstar_b200.offline import OfflineRedepth
     from open_source_einstar_b200.serving import pinned_empty
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
     W_, H_, D_ = 1280, 1024, 256
-    n = args.recording_frames
     rec = synth.recording(n_frames=n, seed=rank, width=W_, height=H_, num_disparities=D_, device=dev)
     lefts, rights = pinned_empty((n, H_, W_), np.uint8), pinned_empty((n, H_, W_), np.uint8)
     for i in range(n):
@@ -448,8 +461,8 @@ def run_offline(args, world, rank, local):
     kernel = Autotuner().tune(FrameKind.of(W_, H_, sp), batch=True)
     out_u16 = pinned_empty((n, H_, W_), np.uint16)
     out_depth = pinned_empty((n, H_, W_), np.float32)
-    with OfflineRedepth(W_, H_, sp, rec.maps, (W_, H_), geom, batch_size=args.offline_batch, kernel=kernel) as off:
-        warm = min(n, 2 * args.offline_batch)
+    with OfflineRedepth(W_, H_, sp, rec.maps, (W_, H_), geom, batch_size=batch, kernel=kernel) as off:
+        warm = min(n, 2 * batch)
         off.run(lefts[:warm], rights[:warm], out_u16[:warm], out_depth[:warm])
         clk = ClockSampler(local).__enter__()
         st = off.run(lefts, rights, out_u16, out_depth)
@@ -468,22 +481,20 @@ def run_offline(args, world, rank, local):
     hbm, hbm_kind = peaks()
     ms = st.device_ms
     formula = algorithmic_bytes(W_, H_, D_, 8, c_b=2, raw=True) * n
-    if rank == 0:
-        line = {"metric": "offline re-depth Gpix*disp/s, 8-path D=256 u16, batches of 128 raw 1280x1024 frames",
-                "workload": "offline", "value": n * W_ * H_ * D_ / (ms * 1e-3) / 1e9, "unit": UNIT,
-                "higher_is_better": True, "n_gpus": world, "frames": n, "batches": st.batches,
-                "frames_per_s": n / (ms * 1e-3), "ms_per_frame": ms / n,
-                "pipeline_frac": formula / (ms * 1e-3) / 1e9 / hbm, "pipeline_formula_bytes_per_frame": formula // n,
-                "peak_gbs": hbm, "peak_kind": hbm_kind, "device_bytes": dev_bytes, "kernel": kernel,
-                "dtype": "u16", "data": "synthetic",
-                "config": {"workload": f"synthetic handheld recording of {n} raw 1280x1024 IR pairs (12-primitive 150 mm "
-                                       "object on a base plane, 250-450 mm standoff, speckle, sigma 2 DN); GPU remap, "
-                                       "8-path SGM D=256 with u16 path values, WTA, L-R, median, u16 + depth; "
-                                       "timed: H2D + batched graph replays + D2H, double-buffered",
-                           "batch": args.offline_batch, "parallelism": f"replicas x{world}"},
-                "clocks": clk.summary()}
-        print(json.dumps(line), flush=True)
-    return 0
+    line = {"metric": f"offline re-depth Gpix*disp/s, 8-path D=256 u16, batches of {batch} raw 1280x1024 frames",
+            "workload": "offline", "value": n * W_ * H_ * D_ / (ms * 1e-3) / 1e9, "unit": UNIT,
+            "higher_is_better": True, "n_gpus": world, "frames": n, "batches": st.batches,
+            "frames_per_s": n / (ms * 1e-3), "ms_per_frame": ms / n,
+            "pipeline_frac": formula / (ms * 1e-3) / 1e9 / hbm, "pipeline_formula_bytes_per_frame": formula // n,
+            "peak_gbs": hbm, "peak_kind": hbm_kind, "device_bytes": dev_bytes, "kernel": kernel,
+            "dtype": "u16", "data": "synthetic",
+            "config": {"workload": f"synthetic handheld recording of {n} raw 1280x1024 IR pairs (12-primitive 150 mm "
+                                   "object on a base plane, 250-450 mm standoff, speckle, sigma 2 DN); GPU remap, "
+                                   "8-path SGM D=256 with u16 path values, WTA, L-R, median, u16 + depth; "
+                                   "timed: H2D + batched graph replays + D2H, double-buffered",
+                       "batch": batch, "parallelism": f"replicas x{world}"},
+            "clocks": clk.summary()}
+    return line
 
 
 def frontend_params(f, baseline):
@@ -678,6 +689,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="default line without the serving and 64-pair batch summaries (single-GPU runs carry them)")
     ap.add_argument("--extras-duration", type=float, default=3.0, help="serving summary: seconds of arrivals per rate")
+    ap.add_argument("--extras-offline-frames", type=int, default=64,
+                    help="offline summary on the default line: frames of the synthetic recording (two batches)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -876,8 +889,9 @@ def main():
     batch.close()
     s.close()
     if world == 1 and not args.no_extras:
-        # configurations 4 and 3 on the same box: the request server under Poisson arrivals (a shorter run per
-        # rate than --workload serving) and the 64-pair uneven batch against per-frame launches
+        # configurations 4, 3 and 5 on the same box: the request server under Poisson arrivals (a shorter run per
+        # rate than --workload serving), the 64-pair uneven batch against per-frame launches, and a 64-frame
+        # offline re-depth (8 paths, D=256, u16 path values; --workload offline runs the longer recording)
         srv = serving_line(dev, args.rates, args.extras_duration, args.slots)
         line["serving"] = {"rates": srv["rates"], "worst_p99_ms": srv["value"], "slots": srv["config"]["slots"],
                            "seconds_per_rate": args.extras_duration, "clocks": srv["clocks"]}
@@ -885,6 +899,10 @@ def main():
         line["batch64"] = {k: b64[k] for k in ("value", "unit", "ms_per_step", "per_frame", "batched_over_per_frame",
                                                "pipeline_frac", "schedule", "launches_per_run", "kernels", "clocks")}
         line["batch64"]["bit_exact_vs_per_frame"] = True  # batch64_line stops the run otherwise
+        off = offline_line(dev, args.extras_offline_frames, args.extras_offline_frames // 2, world, rank, local)
+        line["offline"] = {k: off[k] for k in ("value", "unit", "frames", "batches", "frames_per_s", "ms_per_frame",
+                                               "pipeline_frac", "peak_kind", "kernel", "clocks")}
+        line["offline"]["spot_checked_vs_per_frame"] = True  # offline_line stops the run otherwise
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
