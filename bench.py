@@ -805,7 +805,7 @@ def main():
     # the first copy in to the last copy out.
     from open_source_einstar_b200.offline import OfflineRedepth
     from open_source_einstar_b200.serving import pinned_empty
-    e2e_steps = max(2, args.steps // 2)
+    e2e_steps = max(2, args.steps)  # the K steps of the device-timed region, through the host API
     n_e2e = B * e2e_steps
     host_l, host_r = pinned_empty((B, H, W), np.uint8), pinned_empty((B, H, W), np.uint8)
     for i, p in enumerate(pairs):
