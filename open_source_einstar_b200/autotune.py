@@ -13,7 +13,8 @@ The knobs (ds_kernel_config in include/depth_cuda.h):
 - materialize_costs: write the cost volume once and read it per direction, or recompute each cost
   from the census words in every direction.
 - prefetch_steps: steps of cost / census input kept in flight per scanline (4 or 8).
-- wta_threads: threads per winner-takes-all block.
+- wta_threads: threads per winner-takes-all block (the per-pixel WTA; frames that the row-sweep WTA runs,
+  4 paths with byte values and a 48/64/96/128-disparity slab, skip this stage).
 - fused_pairs (4 directions): the two sweep kernels instead of cost / path / WTA kernels: the vertical path
   pair, then the horizontal pair with the WTA and the L-R check. They need byte pair sums
   (2 (window + P2) <= 255), census windows of at most 32 neighbours and D <= 128, with 4 or 8 lanes per
@@ -65,6 +66,11 @@ class FrameKind:
         return FrameKind(int(width), int(height), int(s.num_disparities), bool(s.eight_paths), wide, window,
                          not wide and 2 * (window + s.p2) <= 255)
 
+    def row_wta_fit(self, dp: int) -> bool:
+        """Whether the library runs the WTA of this kind of frame as row sweeps (k_wta_rows, wta_rows_fit):
+        4 paths, byte pair sums and a lane slab of 48, 64, 96 or 128 disparities."""
+        return not self.eight_paths and self.byte_pair_sums and dp in (48, 64, 96, 128)
+
     def sweep_fit(self) -> bool:
         """Whether the sweep kernels can run this kind of frame (the library's own check, sweep_unfit)."""
         return (not self.eight_paths and self.byte_pair_sums and self.census_window - 1 <= 32
@@ -108,6 +114,8 @@ def stage_candidates(kind: FrameKind, stage: int, best: dict | None = None, fuse
         return [best]  # the sweep kernels have fixed block shapes
     if stage == 2:
         return [{**best, "path_warps_per_block": pw, "prefetch_steps": pf} for pw in (1, 2, 4, 8) for pf in (4, 8)]
+    if kind.row_wta_fit(best["regs_per_lane"] * 2 * best["lanes_per_line"]):
+        return [best]  # the row-sweep WTA runs these frames with a fixed block shape
     return [{**best, "wta_threads": t} for t in (128, 256)]
 
 

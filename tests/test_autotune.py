@@ -19,7 +19,7 @@ def test_tile_shapes_cover_the_disparities_with_least_padding(d):
 
 
 def test_staged_search_finds_the_fastest_of_each_stage():
-    kind = FrameKind(1280, 1024, 128)
+    kind = FrameKind(1280, 1024, 128, eight_paths=True)  # the per-pixel WTA: its block size is searched too
     # a synthetic cost model: SEG 16 R4 materialised, 8 warps, prefetch 8, 128-thread WTA is fastest
     def cost(c):
         ms = 1.0
@@ -36,6 +36,12 @@ def test_staged_search_finds_the_fastest_of_each_stage():
     assert info["ms"] == pytest.approx(1.0)
     n = sum(len(v) for v in info["trials"].values())
     assert n <= 30  # staged: two shapes go through the block search, not the full product (~100)
+    # 4 paths, byte values, a 128-disparity slab: the row-sweep WTA, whose block shape is fixed
+    row = FrameKind(1280, 1024, 128)
+    best4 = {**best, "fused_pairs": 0}
+    assert row.row_wta_fit(128) and stage_candidates(row, 3, best4) == [best4]
+    slab192 = {**best4, "regs_per_lane": 3, "lanes_per_line": 32}
+    assert not row.row_wta_fit(192) and len(stage_candidates(row, 3, slab192)) == 2
 
 
 @pytest.mark.parametrize("d", [4, 24, 40, 48, 64, 96, 128])
