@@ -196,6 +196,8 @@ DS_API uint64_t ds_kernel_launches(void);
  * instead: the vertical path pair, then the horizontal pair with the WTA and the L-R check (two launches
  * per frame, 8 bytes of volume traffic per pixel and disparity). They need 4 paths, census windows of at
  * most 32 neighbours, 2 (window + P2) <= 255, and 4 or 8 lanes per line with regs 6 or 8 (D <= 128).
+ * Otherwise, frames with 4 paths, byte path values (2 (window + P2) <= 255) and a slab of 64, 96 or 128
+ * disparities take the row-sweep WTA, whose block shape is fixed (wta_threads applies to the others).
  * Results are identical for every configuration; only speed differs (the autotuner chooses). */
 typedef struct ds_kernel_config {
     int regs_per_lane;
